@@ -1,0 +1,73 @@
+"""ctypes front end of the libopus chain-decode oracle (oracle/ref_driver.c).
+
+TEST INFRASTRUCTURE.  decode_chains() runs the reference's vendored libopus
+1.5.2 FIXED_POINT decoder with a fresh decoder per chain and returns, per chain,
+the int16 PCM, per-packet sample counts and final ranges, and the stop status.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .corpus import ref_lib
+
+
+def flatten(packets):
+    """bytes blob + uint64 offsets + uint32 lengths of a packet list."""
+    lens = np.array([len(p) for p in packets], dtype=np.uint32)
+    off = np.zeros(len(packets), dtype=np.uint64)
+    if len(packets) > 1:
+        off[1:] = np.cumsum(lens[:-1], dtype=np.uint64)
+    blob = np.frombuffer(b"".join(packets) or b"\0", dtype=np.uint8).copy()
+    return blob, off, lens
+
+
+def decode_chains(packets, chains, channels, nthreads=None, want_pcm=True):
+    """chains: sequence of (first, npkts[, trim, keep]) over `packets`.
+
+    Returns dict(pcm=list of int16 arrays (interleaved), nsamp=list of uint32
+    arrays, rng=list of uint32 arrays, status=int32 array, samples=uint64 array)."""
+    lib = ref_lib()
+    blob, off, lens = flatten(packets)
+    first = np.array([c[0] for c in chains], dtype=np.uint32)
+    npk = np.array([c[1] for c in chains], dtype=np.uint32)
+    nch = len(chains)
+    rec_off = np.zeros(nch, dtype=np.uint64)
+    if nch > 1:
+        rec_off[1:] = np.cumsum(npk[:-1], dtype=np.uint64)
+    cap = np.array([sum(_toc(packets[int(first[i]) + k]) for k in range(int(npk[i])))
+                    for i in range(nch)], dtype=np.uint64)
+    pcm_off = np.zeros(nch, dtype=np.uint64)
+    if nch > 1:
+        pcm_off[1:] = np.cumsum(cap[:-1] * channels, dtype=np.uint64)
+    total = int(cap.sum()) * channels
+    pcm = np.zeros(max(total, 1), dtype=np.int16) if want_pcm else None
+    nrec = int(npk.sum())
+    nsamp = np.zeros(max(nrec, 1), dtype=np.uint32)
+    rng = np.zeros(max(nrec, 1), dtype=np.uint32)
+    status = np.zeros(max(nch, 1), dtype=np.int32)
+    samples = np.zeros(max(nch, 1), dtype=np.uint64)
+    rc = lib.oref_decode_chains(
+        blob.ctypes.data, off.ctypes.data, lens.ctypes.data, first.ctypes.data,
+        npk.ctypes.data, nch, channels,
+        pcm.ctypes.data if want_pcm else None, pcm_off.ctypes.data, rec_off.ctypes.data,
+        nsamp.ctypes.data, rng.ctypes.data, status.ctypes.data, samples.ctypes.data,
+        nthreads or (os.cpu_count() or 1))
+    if rc != 0:
+        raise RuntimeError("oref_decode_chains failed to start threads")
+    out = dict(status=status[:nch], samples=samples[:nch], pcm=[], nsamp=[], rng=[])
+    for i in range(nch):
+        r0, r1 = int(rec_off[i]), int(rec_off[i]) + int(npk[i])
+        out["nsamp"].append(nsamp[r0:r1])
+        out["rng"].append(rng[r0:r1])
+        if want_pcm:
+            p0 = int(pcm_off[i])
+            out["pcm"].append(pcm[p0:p0 + int(samples[i]) * channels])
+    return out
+
+
+def _toc(p):
+    from .ogg_port import toc_samples48
+    return toc_samples48(p)

@@ -1,0 +1,196 @@
+/* Oracle driver over the reference's vendored libopus 1.5.2 (FIXED_POINT).
+ *
+ * TEST INFRASTRUCTURE ONLY.  Linked into oracle/_ref/libopus_ref.so together
+ * with the vendored libopus objects.  The product never loads this library.
+ *
+ * 1. oref_decode_chains: the bit-exactness oracle.  Every chain gets a FRESH
+ *    OpusDecoder(48000, channels) and decodes its packet range in order with
+ *    opus_decode(..., frame_size=5760, decode_fec=0) -- the chain protocol of the
+ *    reference's decode kernel (cuopus_kernels.cuh:41-69, a fresh
+ *    cu_opus_decoder_init per chain, then cu_opus_decode per packet) checked
+ *    against libopus in harness2.cu:200-253.  Per packet it records the sample
+ *    count and OPUS_GET_FINAL_RANGE; per chain the stop status and sample total.
+ *    Chains run on a pthread pool (dynamic assignment) so the same entry point
+ *    is the timed CPU baseline.
+ *
+ * 2. oref_encode: the corpus encoder.  Drives the vendored encoder frame by
+ *    frame at 48 kHz with per-segment forced mode / bandwidth / frame size /
+ *    bitrate (OPUS_SET_FORCE_MODE is the private request 11002 of
+ *    src/opus_private.h:141; per-frame switching follows the idea of
+ *    src/opus_demo.c:820-872).  It keeps encoding zero-padded frames until the
+ *    packets cover pre-skip + input length, so an Ogg muxer can express the
+ *    exact end trim (RFC 7845 sec. 4.4).
+ */
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "opus.h"
+
+#define OREF_FORCE_MODE_REQUEST 11002   /* src/opus_private.h:141 */
+#define OREF_MAX_PKT_SAMPLES 5760       /* 120 ms at 48 kHz */
+
+/* ------------------------------------------------------------------ decode */
+
+typedef struct {
+    const uint8_t *data;
+    const uint64_t *off;
+    const uint32_t *len;
+    const uint32_t *first;
+    const uint32_t *npkts;
+    const uint64_t *rec_off;    /* per chain: index of its first per-packet record */
+    const uint64_t *pcm_off;    /* per chain: int16 element offset into pcm */
+    int nchains, channels;
+    int16_t *pcm;               /* may be NULL: decode into scratch only */
+    uint32_t *pkt_nsamp;        /* per record (may be NULL) */
+    uint32_t *pkt_rng;          /* per record (may be NULL) */
+    int32_t *chain_status;      /* per chain: 0 or first negative opus_decode return */
+    uint64_t *chain_samples;    /* per chain: samples per channel decoded */
+    volatile int next;
+    pthread_mutex_t mu;
+} oref_job;
+
+static void *oref_worker(void *arg)
+{
+    oref_job *j = (oref_job *)arg;
+    int err = 0;
+    OpusDecoder *dec = (OpusDecoder *)malloc((size_t)opus_decoder_get_size(j->channels));
+    int16_t *scratch = (int16_t *)malloc(sizeof(int16_t) * OREF_MAX_PKT_SAMPLES * j->channels);
+    if (!dec || !scratch) { free(dec); free(scratch); return NULL; }
+    for (;;) {
+        pthread_mutex_lock(&j->mu);
+        int c = j->next++;
+        pthread_mutex_unlock(&j->mu);
+        if (c >= j->nchains) break;
+        err = opus_decoder_init(dec, 48000, j->channels);
+        int32_t status = err;
+        uint64_t total = 0;
+        if (!err) {
+            for (uint32_t k = 0; k < j->npkts[c]; k++) {
+                uint64_t p = (uint64_t)j->first[c] + k;
+                int16_t *out = j->pcm ? j->pcm + j->pcm_off[c] + total * (uint64_t)j->channels
+                                      : scratch;
+                int ret = opus_decode(dec, j->data + j->off[p], (opus_int32)j->len[p], out,
+                                      OREF_MAX_PKT_SAMPLES, 0);
+                uint64_t r = j->rec_off ? j->rec_off[c] + k : 0;
+                if (ret < 0) {
+                    status = ret;
+                    if (j->pkt_nsamp) j->pkt_nsamp[r] = 0;
+                    if (j->pkt_rng) j->pkt_rng[r] = 0;
+                    break;
+                }
+                opus_uint32 rng = 0;
+                opus_decoder_ctl(dec, OPUS_GET_FINAL_RANGE(&rng));
+                if (j->pkt_nsamp) j->pkt_nsamp[r] = (uint32_t)ret;
+                if (j->pkt_rng) j->pkt_rng[r] = (uint32_t)rng;
+                total += (uint64_t)ret;
+            }
+        }
+        if (j->chain_status) j->chain_status[c] = status;
+        if (j->chain_samples) j->chain_samples[c] = total;
+    }
+    free(dec);
+    free(scratch);
+    return NULL;
+}
+
+/* Decode nchains chains; returns 0, or -1 when a thread could not start. */
+int oref_decode_chains(const uint8_t *data, const uint64_t *off, const uint32_t *len,
+                       const uint32_t *first, const uint32_t *npkts, int nchains,
+                       int channels, int16_t *pcm, const uint64_t *pcm_off,
+                       const uint64_t *rec_off, uint32_t *pkt_nsamp, uint32_t *pkt_rng,
+                       int32_t *chain_status, uint64_t *chain_samples, int nthreads)
+{
+    oref_job j;
+    memset(&j, 0, sizeof(j));
+    j.data = data; j.off = off; j.len = len; j.first = first; j.npkts = npkts;
+    j.rec_off = rec_off; j.pcm_off = pcm_off; j.nchains = nchains; j.channels = channels;
+    j.pcm = pcm; j.pkt_nsamp = pkt_nsamp; j.pkt_rng = pkt_rng;
+    j.chain_status = chain_status; j.chain_samples = chain_samples;
+    j.next = 0;
+    pthread_mutex_init(&j.mu, NULL);
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 1024) nthreads = 1024;
+    pthread_t th[1024];
+    int started = 0, rc = 0;
+    for (int t = 0; t < nthreads; t++) {
+        if (pthread_create(&th[t], NULL, oref_worker, &j) != 0) { rc = -1; break; }
+        started++;
+    }
+    if (started == 0) oref_worker(&j);
+    for (int t = 0; t < started; t++) pthread_join(th[t], NULL);
+    pthread_mutex_destroy(&j.mu);
+    return rc;
+}
+
+/* ------------------------------------------------------------------ encode */
+
+typedef struct {
+    int64_t start;      /* first input sample (per channel) of the segment */
+    int32_t mode;       /* 1000 SILK, 1001 hybrid, 1002 CELT, -1000 = auto */
+    int32_t bandwidth;  /* OPUS_BANDWIDTH_* or -1000 = auto */
+    int32_t frame_size; /* samples at 48 kHz: 120 240 480 960 1920 2880 */
+    int32_t bitrate;    /* bits per second */
+    int32_t force_channels; /* -1000 auto, 1 or 2 */
+} oref_seg;
+
+/* Encode n samples per channel of interleaved pcm.  Writes packets back to back
+ * into out (capacity out_cap bytes) and their lengths into pkt_len (capacity
+ * max_pkts).  Returns the packet count, or a negative value on error.
+ * *preskip receives OPUS_GET_LOOKAHEAD. */
+int oref_encode(const int16_t *pcm, int64_t n, int channels, const oref_seg *segs,
+                int nsegs, int application, int complexity, int vbr,
+                uint8_t *out, uint64_t out_cap, uint32_t *pkt_len, int max_pkts,
+                int *preskip)
+{
+    int err = 0;
+    OpusEncoder *enc = opus_encoder_create(48000, channels, application, &err);
+    if (!enc || err) return -1000 + err;
+    opus_encoder_ctl(enc, OPUS_SET_COMPLEXITY(complexity));
+    opus_encoder_ctl(enc, OPUS_SET_VBR(vbr));
+    opus_encoder_ctl(enc, OPUS_SET_INBAND_FEC(0));
+    opus_encoder_ctl(enc, OPUS_SET_DTX(0));
+    opus_encoder_ctl(enc, OPUS_SET_PACKET_LOSS_PERC(0));
+    int la = 0;
+    opus_encoder_ctl(enc, OPUS_GET_LOOKAHEAD(&la));
+    if (preskip) *preskip = la;
+
+    int16_t frame[2880 * 2];
+    int64_t pos = 0, covered = 0;
+    uint64_t w = 0;
+    int np = 0, si = -1;
+    while (covered < (int64_t)la + n) {
+        /* segment in force at the current input position */
+        int s = 0;
+        while (s + 1 < nsegs && segs[s + 1].start <= pos) s++;
+        if (s != si) {
+            si = s;
+            opus_encoder_ctl(enc, OREF_FORCE_MODE_REQUEST, (opus_int32)segs[s].mode);
+            opus_encoder_ctl(enc, OPUS_SET_BANDWIDTH(segs[s].bandwidth));
+            opus_encoder_ctl(enc, OPUS_SET_BITRATE(segs[s].bitrate));
+            opus_encoder_ctl(enc, OPUS_SET_FORCE_CHANNELS(segs[s].force_channels));
+        }
+        int fs = segs[s].frame_size;
+        for (int i = 0; i < fs; i++)
+            for (int ch = 0; ch < channels; ch++) {
+                int64_t at = pos + i;
+                frame[i * channels + ch] = at < n ? pcm[at * channels + ch] : 0;
+            }
+        if (np >= max_pkts) { opus_encoder_destroy(enc); return -2000; }
+        uint64_t room = out_cap - w;
+        if (room > 1500) room = 1500;
+        int nb = opus_encode(enc, frame, fs, out + w, (opus_int32)room);
+        if (nb < 0) { opus_encoder_destroy(enc); return -3000 + nb; }
+        pkt_len[np++] = (uint32_t)nb;
+        w += (uint64_t)nb;
+        pos += fs;
+        covered += fs;
+        if (out_cap - w < 1500) { opus_encoder_destroy(enc); return -4000; }
+    }
+    opus_encoder_destroy(enc);
+    return np;
+}
+
+/* libopus version string of the oracle build, for logs. */
+const char *oref_version(void) { return opus_get_version_string(); }
