@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Benchmark of the batched Opus decoder: audio-seconds decoded per second.
+
+Workload (default): the mixed-mode uneven batch - 4096 seeded synthetic Ogg Opus
+streams with log-uniform lengths 1-30 s, forced SILK / hybrid / CELT segments
+of 0.5-3 s, frames 2.5-60 ms, 6-128 kbps, mono or stereo; one chain per stream
+(4096 chains), decoded bit-exactly to int16 48 kHz PCM.  The reference's
+corpora are private; the streams are generated by the vendored libopus encoder
+(oracle/corpus.py) before anything is timed.
+
+A step is one decode of the whole batch.
+  value   device-resident: packets and chain tables already in HBM, one call of
+          the engine (cuopus_decode_batch), CUDA-event timed on its stream.
+  e2e     through the public C ABI (cuopus_decode_i16_multi) from host Ogg
+          bytes: demux, host->device copy, decode, and a device->host read of
+          all decoded PCM into pinned memory, every step.
+  cpu_baseline  libopus 1.5.2 fixed point (the reference's CPU decoder, built
+          from its vendored sources) on all host cores, bounded sample.
+--impl reference runs only that CPU decoder (the reference arm).
+
+Under torchrun every rank decodes its own copy of the batch (weak scaling, no
+data exchange); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (corpus kind, count, max seconds, chain segment seconds)
+    "mixed4096": ("mixed", 4096, 30.0, 1e9),
+    "plain64": ("plain64", 64, 1.0, 1.0),
+    "long7200": ("long", 1, 7200.0, 1.0),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ------------------------------------------------------------------ inputs
+
+def load_inputs(workload, count=None):
+    """Input preparation (never timed): generate or reuse the cached corpus."""
+    from oracle.corpus import build_corpus
+    kind, n, secs, seg = WORKLOADS[workload]
+    t = time.time()
+    paths = build_corpus(kind if kind != "plain64" else "plain64", os.path.join(ROOT, "corpus"),
+                         count=count or n, seconds=secs if kind != "plain64" else None)
+    files = [open(p, "rb").read() for p in paths]
+    log("corpus %s: %d files, %.1f MB, %.1fs" % (workload, len(files), sum(map(len, files)) / 1e6,
+                                                 time.time() - t))
+    return files, seg
+
+
+class DeviceBatch:
+    """Packets + chain table of all files, resident on the device."""
+
+    def __init__(self, files, seg, device):
+        import torch
+        from cuopus_b200 import cuopus_native as cn
+        blobs, offs, lens, first, npk, chans, trim, keep = [], [], [], [], [], [], [], []
+        base_b = 0
+        base_p = 0
+        self.audio_s = 0.0
+        self.pkt_bytes = 0
+        self.pcm_bytes = 0
+        for f in files:
+            ix = cn.index(f, seg_s=seg, preroll_ms=250.0)
+            blobs.append(ix.blob)
+            offs.append(ix.pkt_off + base_b)
+            lens.append(ix.pkt_len)
+            first.append(ix.first + base_p)
+            npk.append(ix.npkts)
+            chans.append(np.full(len(ix.first), ix.channels, np.uint8))
+            trim.append(ix.trim.astype(np.uint64))
+            keep.append(ix.keep.astype(np.uint64))
+            base_b += len(ix.blob)
+            base_p += len(ix.pkt_len)
+            self.audio_s += ix.play48 / 48000.0
+            self.pcm_bytes += int(ix.play48) * ix.channels * 2
+            # packet bytes decoded, preroll packets included
+            for c in range(len(ix.first)):
+                a, b = int(ix.first[c]), int(ix.first[c]) + int(ix.npkts[c])
+                self.pkt_bytes += int(ix.pkt_len[a:b].sum())
+        cat = lambda xs: np.ascontiguousarray(np.concatenate(xs))
+        first, npk, chans = cat(first), cat(npk), cat(chans)
+        trim, keep = cat(trim), cat(keep)
+        out_off = np.zeros(len(first), np.uint64)
+        out_off[1:] = np.cumsum(keep[:-1] * chans[:-1].astype(np.uint64))
+        self.n = len(first)
+        self.cap_pkts = npk
+        self.chans = chans
+        self.keep = keep
+        tot = int((keep * chans.astype(np.uint64)).sum())
+        dev = torch.device(device)
+        T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        self.t = dict(blob=T(np.concatenate(blobs + [np.zeros(16, np.uint8)])), off=T(cat(offs)),
+                      len=T(cat(lens)), first=T(first), npkts=T(npk), chans=T(chans), trim=T(trim),
+                      keep=T(keep), out_off=T(out_off))
+        self.out = torch.empty(max(tot, 1), dtype=torch.int16, device=dev)
+        self.res = torch.zeros(4 * self.n, dtype=torch.int32, device=dev)
+
+    def batch(self, width, schedule, order=None):
+        from cuopus_b200 import cuopus_native as cn
+        b = cn.Batch()
+        t = self.t
+        b.data, b.off, b.len = t["blob"].data_ptr(), t["off"].data_ptr(), t["len"].data_ptr()
+        b.first, b.npkts, b.channels = t["first"].data_ptr(), t["npkts"].data_ptr(), t["chans"].data_ptr()
+        b.trim, b.keep, b.out_off = t["trim"].data_ptr(), t["keep"].data_ptr(), t["out_off"].data_ptr()
+        b.out, b.res = self.out.data_ptr(), self.res.data_ptr()
+        b.nchains, b.width, b.schedule, b.max_groups = self.n, width, schedule, 0
+        self._order = None
+        if order is not None:
+            self._order = np.ascontiguousarray(np.asarray(order, np.uint32))
+            b.order = self._order.ctypes.data
+        return b
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return None
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ CPU (oracle) decode
+
+def cpu_decode(files, seg, budget_s, threads):
+    """libopus on host threads over a prefix of the workload; returns
+    (audio-s/s, audio seconds decoded, seconds, files used)."""
+    from oracle import ogg_port, ref_decode
+    t_all = time.time()
+    audio = 0.0
+    used = 0
+    elapsed = 0.0
+    # decode in groups so the sample stays bounded by the time budget
+    group = max(threads * 4, 16)
+    while used < len(files) and elapsed < budget_s:
+        chunk = files[used:used + group]
+        pk_all, ch_all, chains_all = [], [], []
+        for f in chunk:
+            ix = ogg_port.demux(f)
+            pk_all.append(ix["packets"])
+            ch_all.append(ix["channels"])
+            chains_all.append(ogg_port.build_chains(ix, seg, 250.0))
+            audio_f = ix["play48"] / 48000.0
+            audio += audio_f
+        t0 = time.time()
+        # one oracle call per channel count (chains of a call share it)
+        for want_ch in (1, 2):
+            pk, chains = [], []
+            base = 0
+            for p, ch, cs in zip(pk_all, ch_all, chains_all):
+                if ch != want_ch:
+                    continue
+                pk += p
+                chains += [(c[0] + base, c[1], c[2], c[3]) for c in cs]
+                base += len(p)
+            if chains:
+                ref_decode.decode_chains(pk, chains, want_ch, nthreads=threads)
+        elapsed += time.time() - t0
+        used += len(chunk)
+    return audio / elapsed if elapsed > 0 else 0.0, audio, elapsed, used
+
+
+# ------------------------------------------------------------------ main
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mixed4096", choices=sorted(WORKLOADS))
+    ap.add_argument("--count", type=int, default=None, help="override the stream count (development)")
+    ap.add_argument("--width", type=int, default=int(os.environ.get("CUOPUS_STRIDE", "32")))
+    ap.add_argument("--schedule", default="queue", choices=["queue", "static"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        files, seg = load_inputs(args.workload, args.count)
+        rates = []
+        for i in range(args.warmup + args.steps):
+            r, audio, el, used = cpu_decode(files, seg, args.cpu_budget / 2, threads)
+            if i >= args.warmup:
+                rates.append(r)
+        v = statistics.median(rates)
+        line = {"metric": "audio-sec decoded/sec on 1 B200 (bit-exact)", "value": v, "unit": "audio-s/s",
+                "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "int16", "data": "synthetic (seeded, vendored libopus encoder)",
+                "config": {"workload": args.workload, "chains": None, "sample_files": used},
+                "cpu_baseline": {"value": v, "unit": "audio-s/s", "cores": threads, "kind": "reference",
+                                 "sample": "first %d streams (%.0f audio-s) per step" % (used, audio)},
+                "e2e": {"value": v, "unit": "audio-s/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = "cuda:%d" % local
+    from cuopus_b200 import cuopus_native as cn
+
+    files, seg = load_inputs(args.workload, args.count)
+    db = DeviceBatch(files, seg, dev)
+    cn.warmup()
+    sched = 1 if args.schedule == "queue" else 0
+    order = None
+    if sched == 1:
+        # longest first: packets x channels as the cost proxy
+        order = np.argsort(-(db.cap_pkts.astype(np.int64) * db.chans), kind="stable")
+    b = db.batch(args.width, sched, order)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        cn.decode_batch(b, stream.cuda_stream)
+    res = db.res.view(-1, 4).cpu().numpy()
+    bad = int((res[:, 0] != 0).sum())
+    if bad:
+        log("WARNING: %d chains stopped with a decode error" % bad)
+    barrier()
+    torch.cuda.synchronize()
+    kern = []
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            kern.append(cn.decode_batch(b, stream.cuda_stream))
+        e1.record(stream)
+        torch.cuda.synchronize()
+    step_ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([step_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms = float(t.item())
+    barrier()
+    value = world * db.audio_s / (step_ms / 1e3)
+    kern_ms = statistics.mean(kern)
+    alg_bytes = db.pkt_bytes + db.pcm_bytes
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg_bytes / (kern_ms / 1e3) / 1e9
+
+    # e2e through the C ABI from host bytes, PCM read back to pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        play = [cn.probe_pcm(f) for f in files]
+        caps = [p * c for p, c in play]
+        outs = [torch.empty(max(c, 1), dtype=torch.int16, device=dev) for c in caps]
+        host = torch.empty(max(sum(caps), 1), dtype=torch.int16, pin_memory=True)
+        import ctypes
+        lib = cn.lib()
+        n = len(files)
+        ba = (ctypes.c_char_p * n)(*files)
+        la = (ctypes.c_size_t * n)(*[len(f) for f in files])
+        oa = (ctypes.c_void_p * n)(*[o.data_ptr() for o in outs])
+        ca = (ctypes.c_size_t * n)(*caps)
+        ol = (ctypes.c_int64 * n)()
+        oc = (ctypes.c_int32 * n)()
+        err = ctypes.create_string_buffer(512)
+        os.environ["CUOPUS_SEG_S"] = str(seg)
+        os.environ["CUOPUS_MAX_BATCH"] = str(10 ** 8)
+
+        def e2e_step():
+            rc = lib.cuopus_decode_i16_multi(ba, la, n, oa, ca, ol, oc, ctypes.c_void_p(stream.cuda_stream),
+                                             err, 512)
+            if rc:
+                raise RuntimeError(err.value.decode())
+            o = 0
+            for t_, c in zip(outs, caps):
+                host[o:o + c].copy_(t_[:c], non_blocking=True)
+                o += c
+            torch.cuda.synchronize()
+
+        for _ in range(2):
+            e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        e2e_s = (time.perf_counter() - t0) / args.steps
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([e2e_s], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": world * db.audio_s / e2e_s, "unit": "audio-s/s",
+               "h2d_bytes_per_step": int(sum(map(len, files))), "d2h_bytes_per_step": int(2 * sum(caps)),
+               "ms_per_step": e2e_s * 1e3}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        r, audio, el, used = cpu_decode(files, seg, args.cpu_budget, threads)
+        cpu = {"value": r, "unit": "audio-s/s", "cores": threads, "kind": "reference",
+               "sample": "libopus 1.5.2 fixed point on %d host threads: first %d of %d streams (%.0f audio-s, %.1fs)"
+                         % (threads, used, len(files), audio, el)}
+
+    if rank == 0:
+        line = {"metric": "audio-sec decoded/sec on 1 B200 (bit-exact)", "value": value, "unit": "audio-s/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16",
+                "data": "synthetic (seeded, vendored libopus encoder)",
+                "config": {"workload": args.workload, "streams": len(files), "chains": db.n,
+                           "audio_s_per_gpu": round(db.audio_s, 1), "width": args.width,
+                           "schedule": args.schedule, "l2": "inputs and outputs exceed L2 (no flush needed)"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": None,
+                             "alg_bytes_per_launch": alg_bytes, "kernel_ms": kern_ms},
+                "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "gpu_launches": args.steps,
+                "decode_errors": bad}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

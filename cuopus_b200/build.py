@@ -1,0 +1,103 @@
+"""Build recipe of the native libraries (in-tree, so they travel with the repo).
+
+  cuopus_b200/lib/libcuopus.so            the product: CUDA kernels for sm_100a
+                                          plus the C ABI of include/cuopus.h
+  cuopus_b200/lib/libcuopus_hostcheck.so  the same decoder sources compiled for
+                                          the host (g++), used only by tests
+  cuopus_b200/bin/cuopus_decode           the command-line tool / daemon
+
+python -m cuopus_b200.build [--force]
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "lib")
+BIN = os.path.join(HERE, "bin")
+NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+LIBCUOPUS = os.path.join(LIB, "libcuopus.so")
+HOSTCHECK = os.path.join(LIB, "libcuopus_hostcheck.so")
+CLI = os.path.join(BIN, "cuopus_decode")
+
+
+def _sources(*names):
+    out = []
+    for n in names:
+        p = os.path.join(CSRC, n)
+        if os.path.isdir(p):
+            out += [os.path.join(p, f) for f in sorted(os.listdir(p))]
+        else:
+            out.append(p)
+    return out
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def _run(cmd):
+    print("+", " ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build_libcuopus(force=False):
+    deps = _sources("libcuopus.cu", "kernels.cuh", "ogg_demux.cpp", "ogg_demux.h", "dec") + \
+        [os.path.join(ROOT, "include", "cuopus.h")]
+    if not force and not _stale(LIBCUOPUS, deps):
+        return LIBCUOPUS
+    os.makedirs(LIB, exist_ok=True)
+    tmp = LIBCUOPUS + ".tmp"
+    _run([NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xptxas", "-v", "-Xcompiler", "-fPIC,-O2",
+          "-shared", "-I", CSRC, os.path.join(CSRC, "libcuopus.cu"), os.path.join(CSRC, "ogg_demux.cpp"),
+          "-o", tmp])
+    os.replace(tmp, LIBCUOPUS)
+    return LIBCUOPUS
+
+
+def build_hostcheck(force=False):
+    deps = _sources("hostcheck.cpp", "dec")
+    if not force and not _stale(HOSTCHECK, deps):
+        return HOSTCHECK
+    os.makedirs(LIB, exist_ok=True)
+    tmp = HOSTCHECK + ".tmp"
+    _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-w", "-I", CSRC,
+          os.path.join(CSRC, "hostcheck.cpp"), "-o", tmp, "-lpthread"])
+    os.replace(tmp, HOSTCHECK)
+    return HOSTCHECK
+
+
+def build_cli(force=False):
+    src = os.path.join(CSRC, "cli.cpp")
+    if not os.path.exists(src):
+        return None
+    deps = [src, os.path.join(ROOT, "include", "cuopus.h"), LIBCUOPUS]
+    if not force and not _stale(CLI, deps):
+        return CLI
+    os.makedirs(BIN, exist_ok=True)
+    cuda = os.path.dirname(os.path.dirname(NVCC))
+    _run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(cuda, "include"),
+          src, "-o", CLI + ".tmp", "-L", LIB, "-lcuopus", "-Wl,-rpath,$ORIGIN/../lib",
+          "-L", os.path.join(cuda, "lib64"), "-lcudart", "-lpthread"])
+    os.replace(CLI + ".tmp", CLI)
+    return CLI
+
+
+def build_all(force=False):
+    build_libcuopus(force)
+    build_hostcheck(force)
+    build_cli(force)
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv)

@@ -1,0 +1,81 @@
+// Host build of the chain decoder (the same sources as the CUDA kernel,
+// compiled by g++ with one lane per chain).  It is the host same-source
+// check: the CPU parity tests run it against libopus to separate "the
+// restatement is right" from "the CUDA execution is right".  Test-only; the
+// product library never loads it and never falls back to it.
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+
+#include "dec/chain.cuh"
+
+extern "C" {
+
+struct hc_job {
+    const uint8_t *data;
+    const uint64_t *off;
+    const uint32_t *len;
+    const uint32_t *first, *npkts;
+    const int32_t *channels;
+    int16_t *pcm;
+    const uint64_t *pcm_off;
+    const uint64_t *trim, *keep;
+    const uint64_t *rec_off;
+    uint32_t *pkt_nsamp, *pkt_rng;
+    cuo::ChainResult *res;
+    int nchains;
+    int next;
+    pthread_mutex_t mu;
+};
+
+static void *hc_worker(void *arg)
+{
+    hc_job *j = (hc_job *)arg;
+    cuo::ChainSlot *slot = (cuo::ChainSlot *)calloc(1, sizeof(cuo::ChainSlot));
+    if (!slot) return nullptr;
+    cuo::Lanes L{0, 1, 1u};
+    for (;;) {
+        pthread_mutex_lock(&j->mu);
+        int c = j->next++;
+        pthread_mutex_unlock(&j->mu);
+        if (c >= j->nchains) break;
+        uint64_t r = j->rec_off ? j->rec_off[c] : 0;
+        cuo::decode_chain(L, slot, j->data, j->off, j->len, j->first[c], j->npkts[c], j->channels[c],
+                          j->pcm ? j->pcm + j->pcm_off[c] : nullptr, j->trim ? j->trim[c] : 0,
+                          j->keep ? j->keep[c] : (uint64_t)-1 / 4, j->pkt_nsamp ? j->pkt_nsamp + r : nullptr,
+                          j->pkt_rng ? j->pkt_rng + r : nullptr, &j->res[c]);
+    }
+    free(slot);
+    return nullptr;
+}
+
+// Same layout as the oracle's oref_decode_chains, plus per-chain channels and
+// keep windows (trim/keep may be null: keep everything).  res: 4 words per chain.
+int hc_decode_chains(const uint8_t *data, const uint64_t *off, const uint32_t *len, const uint32_t *first,
+                     const uint32_t *npkts, const int32_t *channels, int nchains, int16_t *pcm,
+                     const uint64_t *pcm_off, const uint64_t *trim, const uint64_t *keep, const uint64_t *rec_off,
+                     uint32_t *pkt_nsamp, uint32_t *pkt_rng, void *res, int nthreads)
+{
+    hc_job j;
+    j.data = data; j.off = off; j.len = len; j.first = first; j.npkts = npkts; j.channels = channels;
+    j.pcm = pcm; j.pcm_off = pcm_off; j.trim = trim; j.keep = keep; j.rec_off = rec_off;
+    j.pkt_nsamp = pkt_nsamp; j.pkt_rng = pkt_rng; j.res = (cuo::ChainResult *)res;
+    j.nchains = nchains; j.next = 0;
+    pthread_mutex_init(&j.mu, nullptr);
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    pthread_t th[256];
+    int started = 0;
+    for (int t = 0; t < nthreads; t++) {
+        if (pthread_create(&th[t], nullptr, hc_worker, &j) != 0) break;
+        started++;
+    }
+    if (!started) hc_worker(&j);
+    for (int t = 0; t < started; t++) pthread_join(th[t], nullptr);
+    pthread_mutex_destroy(&j.mu);
+    return 0;
+}
+
+unsigned long hc_slot_bytes(void) { return sizeof(cuo::ChainSlot); }
+
+}

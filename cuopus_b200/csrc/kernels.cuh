@@ -1,0 +1,119 @@
+// Device kernels of libcuopus (sm_100a).
+//
+//   k_decode_chains   one decoder per group of `width` lanes; the groups of a
+//                     launch are resident decoder slots.  Two schedules:
+//                       plain      chain c goes to group c % ngroups (static)
+//                       queue      groups pull chain indices from a device
+//                                  counter in the order given by `order`
+//                                  (longest first when the host sorts it);
+//                                  the loop is bounded by the chain count
+//   k_resample48to16  49-tap Kaiser-windowed sinc, 3:1 decimation of the
+//                     compacted int16 48 kHz stream into fp32 16 kHz: input
+//                     tiles staged in shared memory, each thread emits four
+//                     consecutive outputs as one float4 store.
+//
+// Arithmetic of the resampler follows the reference kernel
+// (cuopus_kernels.cuh:96-111): acc starts at 0 and adds taps[t] * x/32768
+// for t = 0..48 in order with a fused multiply-add, samples outside the
+// stream read as zero.
+#pragma once
+#include "dec/chain.cuh"
+
+namespace cuo {
+
+struct DecodeArgs {
+    const uint8_t *data;        // packet bytes
+    const uint64_t *off;        // per packet offset
+    const uint32_t *len;        // per packet length
+    const uint32_t *first;      // per chain first packet
+    const uint32_t *npkts;      // per chain packet count
+    const uint8_t *channels;    // per chain channel count (1 or 2)
+    const uint64_t *trim;       // per chain samples to drop (per channel)
+    const uint64_t *keep;       // per chain samples to keep (per channel)
+    const uint64_t *out_off;    // per chain int16 element offset into out
+    int16_t *out;               // kept PCM, interleaved
+    const uint32_t *order;      // queue schedule: chain visiting order (may be null)
+    const uint64_t *rec_off;    // per chain first per-packet record (may be null)
+    uint32_t *pkt_nsamp;        // per-packet records (may be null)
+    uint32_t *pkt_rng;
+    ChainResult *res;           // per chain result
+    ChainSlot *slots;           // one per group of the launch
+    unsigned *queue_head;       // queue schedule: next position in `order`
+    int nchains;
+    int width;                  // lanes per chain: 1, 2, 4, 8, 16 or 32
+    int use_queue;
+};
+
+__global__ void __launch_bounds__(128) k_decode_chains(DecodeArgs a)
+{
+    const int W = a.width;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / W;
+    Lanes L;
+    L.id = lane - sub * W;
+    L.n = W;
+    L.mask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << (sub * W));
+    const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int group = (int)(gtid / W);
+    const int ngroups = (int)((long long)gridDim.x * blockDim.x / W);
+    ChainSlot *slot = a.slots + group;
+    for (int it = 0; it < a.nchains; it++) {
+        int pos;
+        if (a.use_queue) {
+            unsigned v = 0;
+            if (L.id == 0) v = atomicAdd(a.queue_head, 1u);
+            v = __shfl_sync(L.mask, v, sub * W);
+            pos = (int)v;
+        } else {
+            pos = group + it * ngroups;
+        }
+        if (pos >= a.nchains) break;
+        int c = a.order ? (int)a.order[pos] : pos;
+        long long t0 = clock64();
+        decode_chain(L, slot, a.data, a.off, a.len, a.first[c], a.npkts[c], a.channels[c],
+                     a.out ? a.out + a.out_off[c] : nullptr, a.trim[c], a.keep[c],
+                     a.pkt_nsamp ? a.pkt_nsamp + a.rec_off[c] : nullptr,
+                     a.pkt_rng ? a.pkt_rng + a.rec_off[c] : nullptr, &a.res[c]);
+        long long t1 = clock64();
+        if (L.id == 0) a.res[c].cycles = (uint32_t)min(t1 - t0, 0xffffffffLL);
+    }
+}
+
+enum { RS_TAPS = 49, RS_PAD = 24, RS_OUT_PER_THREAD = 4, RS_THREADS = 256,
+       RS_TILE_OUT = RS_THREADS * RS_OUT_PER_THREAD, RS_TILE_IN = 3 * RS_TILE_OUT + RS_TAPS - 1 };
+
+__constant__ float c_rs_taps[RS_TAPS];
+
+// out[i] for i in [0, n_out): taps over in[3 i - 24 + t], in valid on [0, avail)
+__global__ void __launch_bounds__(RS_THREADS) k_resample48to16(const int16_t *__restrict__ in, long long avail,
+                                                               long long n_out, float *__restrict__ out)
+{
+    __shared__ float xs[RS_TILE_IN];
+    const long long o0 = (long long)blockIdx.x * RS_TILE_OUT;
+    const long long base = 3 * o0 - RS_PAD;
+    for (int i = threadIdx.x; i < RS_TILE_IN; i += RS_THREADS) {
+        long long g = base + i;
+        xs[i] = (g >= 0 && g < avail) ? (float)in[g] * (1.0f / 32768.0f) : 0.0f;
+    }
+    __syncthreads();
+    const int j0 = threadIdx.x * RS_OUT_PER_THREAD;
+    float acc[RS_OUT_PER_THREAD];
+#pragma unroll
+    for (int k = 0; k < RS_OUT_PER_THREAD; k++) {
+        float a = 0.0f;
+        const float *x = xs + 3 * (j0 + k);
+#pragma unroll
+        for (int t = 0; t < RS_TAPS; t++) a = __fmaf_rn(c_rs_taps[t], x[t], a);
+        acc[k] = a;
+    }
+    long long i0 = o0 + j0;
+    if (i0 + RS_OUT_PER_THREAD <= n_out && ((((uintptr_t)(out + i0)) & 15) == 0)) {
+        *reinterpret_cast<float4 *>(out + i0) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < RS_OUT_PER_THREAD; k++)
+            if (i0 + k < n_out) out[i0 + k] = acc[k];
+    }
+}
+
+} // namespace cuo

@@ -1,0 +1,664 @@
+// libcuopus.so: C ABI of the batch decoder (declarations and the meaning of
+// every entry point: include/cuopus.h).
+//
+// Host orchestration restated from the reference's libcuopus.cu: demux and
+// chain tables on the host, validation of every chain against its TOC
+// capacity before success is returned, RC / errbuf conventions, the refusal
+// to run while the caller's stream captures, grow-only process-global
+// workspaces.  The B200 design differs in how the work is laid out:
+//   * all chains of a call go to one decode launch (no 2048-chain batching
+//     with resampler carries); the launch is sized to the resident decoder
+//     slots of the GPU and chains are assigned statically or pulled from a
+//     device work queue;
+//   * the decode kernel writes only the kept samples, straight into the
+//     compacted stream (no separate compaction kernel, no preroll PCM buffer);
+//   * decoder state and scratch live in per-slot global memory (no per-thread
+//     bump arena), so arena overflow cannot happen.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/cuopus.h"
+#include "kernels.cuh"
+#include "ogg_demux.h"
+
+namespace {
+
+enum { RC_OK = 0, RC_SOFT = 1, RC_CUDA = 2, RC_ARG = 3 };
+const int BLOCK = 128;
+const double SWR_TAIL_48K = 48;   // samples the CPU path never flushes (libcuopus.cu:195-199)
+
+struct Err {
+    char *buf;
+    size_t cap;
+    char scratch[8];
+    Err(char *b, size_t c)
+    {
+        if (b && c) { buf = b; cap = c; }
+        else { buf = scratch; cap = sizeof scratch; }
+        buf[0] = 0;
+    }
+    int set(int rc, const char *fmt, ...)
+    {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, cap, fmt, ap);
+        va_end(ap);
+        return rc;
+    }
+};
+
+#define CK(call)                                                                                    \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return err.set(RC_CUDA, "CUDA error %s at %s:%d: %s", #call, __FILE__, __LINE__,       \
+                           cudaGetErrorString(e_));                                                 \
+    } while (0)
+
+struct Grow {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+struct State {
+    Grow data, off, len, first, npkts, chans, trim, keep, out_off, order, res, slots, queue, pcm;
+    Grow hpin;
+    long long dev_bytes = 0;
+    int taps_dev = -1;
+    int occ_dev = -1, occ_blocks = 0, sm_count = 0;
+    float last_kernel_ms = 0.f;
+    int last_ovf = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int ev_dev = -1;
+} G;
+
+std::mutex g_mu;
+
+int gpu_grow(Grow &g, size_t need, Err &err)
+{
+    if (need == 0) need = 1;
+    if (need <= g.cap) return RC_OK;
+    if (g.p) {
+        cudaFree(g.p);
+        G.dev_bytes -= (long long)g.cap;
+        g.p = nullptr;
+        g.cap = 0;
+    }
+    cudaError_t e = cudaMalloc(&g.p, need);
+    if (e != cudaSuccess) return err.set(RC_CUDA, "cudaMalloc %zu bytes: %s", need, cudaGetErrorString(e));
+    g.cap = need;
+    G.dev_bytes += (long long)need;
+    return RC_OK;
+}
+
+int pin_grow(Grow &g, size_t need, Err &err)
+{
+    if (need == 0) need = 1;
+    if (need <= g.cap) return RC_OK;
+    if (g.p) cudaFreeHost(g.p);
+    g.p = nullptr;
+    g.cap = 0;
+    cudaError_t e = cudaMallocHost(&g.p, need);
+    if (e != cudaSuccess) return err.set(RC_CUDA, "cudaMallocHost %zu bytes: %s", need, cudaGetErrorString(e));
+    g.cap = need;
+    return RC_OK;
+}
+
+double env_f(const char *name, double dflt)
+{
+    const char *e = getenv(name);
+    return (e && *e) ? atof(e) : dflt;
+}
+int env_i(const char *name, int dflt)
+{
+    const char *e = getenv(name);
+    return (e && atoi(e) > 0) ? atoi(e) : dflt;
+}
+
+int default_width()
+{
+    int w = env_i("CUOPUS_STRIDE", 32);
+    int p = 1;
+    while (p * 2 <= w && p < 32) p *= 2;
+    return p;
+}
+
+int refuse_capture(cudaStream_t st, Err &err)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &cs);
+    if (e == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+        return err.set(RC_ARG, "refusing to decode during CUDA stream capture");
+    cudaGetLastError();
+    return RC_OK;
+}
+
+// Kaiser-windowed sinc low-pass at 1/3 of the 48 kHz Nyquist rate, 49 taps,
+// beta 8.6, normalised to unity DC gain; computed in double, rounded to float.
+void make_taps(float *taps)
+{
+    const int n = cuo::RS_TAPS;
+    const double beta = 8.6, cutoff = 1.0 / 3.0;
+    auto i0 = [](double x) {   // modified Bessel function of order 0, power series
+        double sum = 1.0, term = 1.0, q = x * x / 4.0;
+        for (int k = 1; k < 64; k++) {
+            term *= q / ((double)k * k);
+            sum += term;
+            if (term < 1e-18 * sum) break;
+        }
+        return sum;
+    };
+    double h[cuo::RS_TAPS], total = 0.0;
+    for (int i = 0; i < n; i++) {
+        double m = i - (n - 1) / 2.0;
+        double sinc = (m == 0.0) ? cutoff : sin(M_PI * cutoff * m) / (M_PI * m);
+        double r = 2.0 * i / (n - 1) - 1.0;
+        double win = i0(beta * sqrt(1.0 - r * r)) / i0(beta);
+        h[i] = sinc * win;
+        total += h[i];
+    }
+    for (int i = 0; i < n; i++) taps[i] = (float)(h[i] / total);
+}
+
+int ensure_taps(cudaStream_t st, Err &err)
+{
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (G.taps_dev == dev) return RC_OK;
+    float taps[cuo::RS_TAPS];
+    make_taps(taps);
+    CK(cudaMemcpyToSymbolAsync(cuo::c_rs_taps, taps, sizeof taps, 0, cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    G.taps_dev = dev;
+    return RC_OK;
+}
+
+int ensure_occupancy(Err &err)
+{
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (G.occ_dev == dev) return RC_OK;
+    CK(cudaDeviceGetAttribute(&G.sm_count, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&G.occ_blocks, cuo::k_decode_chains, BLOCK, 0));
+    if (G.occ_blocks < 1) G.occ_blocks = 1;
+    G.occ_dev = dev;
+    return RC_OK;
+}
+
+int ensure_events(Err &err)
+{
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (G.ev_dev == dev && G.ev0) return RC_OK;
+    CK(cudaEventCreate(&G.ev0));
+    CK(cudaEventCreate(&G.ev1));
+    G.ev_dev = dev;
+    return RC_OK;
+}
+
+// ------------------------------------------------------------------ engine
+
+int decode_batch(const cuopus_batch *b, cudaStream_t st, float *kernel_ms, Err &err)
+{
+    if (!b) return err.set(RC_ARG, "batch is NULL");
+    if (b->nchains <= 0) return RC_OK;
+    int width = b->width > 0 ? b->width : default_width();
+    if (width != 1 && width != 2 && width != 4 && width != 8 && width != 16 && width != 32)
+        return err.set(RC_ARG, "width %d is not a power of two <= 32", width);
+    if (!b->data || !b->off || !b->len || !b->first || !b->npkts || !b->channels || !b->trim || !b->keep ||
+        !b->res)
+        return err.set(RC_ARG, "batch has a NULL table");
+    if (b->out && !b->out_off) return err.set(RC_ARG, "out without out_off");
+    if ((b->pkt_nsamp || b->pkt_rng) && !b->rec_off) return err.set(RC_ARG, "per-packet records without rec_off");
+    int rc = ensure_occupancy(err);
+    if (rc) return rc;
+    if ((rc = ensure_events(err))) return rc;
+    long long resident = (long long)G.sm_count * G.occ_blocks * (BLOCK / width);
+    long long groups = std::min<long long>(b->nchains, resident);
+    if (b->max_groups > 0) groups = std::min<long long>(groups, b->max_groups);
+    int gpb = BLOCK / width;
+    int blocks = (int)((groups + gpb - 1) / gpb);
+    long long nslots = (long long)blocks * gpb;
+    if ((rc = gpu_grow(G.slots, (size_t)nslots * sizeof(cuo::ChainSlot), err))) return rc;
+    if ((rc = gpu_grow(G.queue, sizeof(unsigned), err))) return rc;
+    const uint32_t *order_dev = nullptr;
+    if (b->schedule == 1 && b->order) {
+        if ((rc = gpu_grow(G.order, 4ull * b->nchains, err))) return rc;
+        CK(cudaMemcpyAsync(G.order.p, b->order, 4ull * b->nchains, cudaMemcpyHostToDevice, st));
+        order_dev = (const uint32_t *)G.order.p;
+    }
+    CK(cudaMemsetAsync(G.queue.p, 0, sizeof(unsigned), st));
+    cuo::DecodeArgs a;
+    a.data = b->data;
+    a.off = b->off;
+    a.len = b->len;
+    a.first = b->first;
+    a.npkts = b->npkts;
+    a.channels = b->channels;
+    a.trim = b->trim;
+    a.keep = b->keep;
+    a.out_off = b->out_off;
+    a.out = b->out;
+    a.order = order_dev;
+    a.rec_off = b->rec_off;
+    a.pkt_nsamp = b->pkt_nsamp;
+    a.pkt_rng = b->pkt_rng;
+    a.res = (cuo::ChainResult *)b->res;
+    a.slots = (cuo::ChainSlot *)G.slots.p;
+    a.queue_head = (unsigned *)G.queue.p;
+    a.nchains = b->nchains;
+    a.width = width;
+    a.use_queue = b->schedule == 1;
+    CK(cudaEventRecord(G.ev0, st));
+    cuo::k_decode_chains<<<blocks, BLOCK, 0, st>>>(a);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(G.ev1, st));
+    if (kernel_ms) {
+        CK(cudaEventSynchronize(G.ev1));
+        CK(cudaEventElapsedTime(kernel_ms, G.ev0, G.ev1));
+        G.last_kernel_ms = *kernel_ms;
+    }
+    return RC_OK;
+}
+
+// One call's worth of files merged into a single chain table.
+struct Plan {
+    std::vector<uint8_t> blob;
+    std::vector<uint64_t> off;
+    std::vector<uint32_t> len;
+    std::vector<uint32_t> first, npkts;
+    std::vector<uint8_t> chans;
+    std::vector<uint64_t> trim, keep, out_off, cap;
+    std::vector<uint64_t> file_out0, file_keep;   // per file: element offset / kept samples per channel
+    std::vector<int> file_chans;
+    std::vector<int64_t> file_play48;
+    uint64_t out_elems = 0;
+};
+
+int plan_files(const uint8_t *const *oggs, const size_t *ns, int nfiles, bool require_mono, Plan &P, Err &err)
+{
+    double seg_s = env_f("CUOPUS_SEG_S", 1.0);
+    double preroll_ms = env_f("CUOPUS_PREROLL_MS", 250.0);
+    for (int f = 0; f < nfiles; f++) {
+        if (!oggs || !ns || !oggs[f] || !ns[f]) return err.set(RC_ARG, "file %d: empty input", f);
+        cuo_host::Demux d;
+        cuo_host::Chains c;
+        std::string e;
+        if (!cuo_host::demux_and_chain(oggs[f], ns[f], seg_s, preroll_ms, require_mono, d, &c, e))
+        {
+            if (nfiles > 1) return err.set(RC_SOFT, "file %d: %s", f, e.c_str());
+            return err.set(RC_SOFT, "%s", e.c_str());
+        }
+        uint64_t pkt_base = P.len.size(), data_base = P.blob.size();
+        P.blob.insert(P.blob.end(), d.blob.begin(), d.blob.end());
+        for (uint32_t k = 0; k < d.n_packets(); k++) {
+            P.off.push_back(d.off[k] + data_base);
+            P.len.push_back(d.len[k]);
+        }
+        uint64_t fkeep = 0;
+        P.file_out0.push_back(P.out_elems);
+        for (uint32_t i = 0; i < c.size(); i++) {
+            uint64_t capn = 0;
+            for (uint32_t k = 0; k < c.npkts[i]; k++) {
+                uint32_t p = c.first[i] + k;
+                capn += (uint64_t)cuo_host::toc_samples48(d.blob.data() + d.off[p], d.len[p]);
+            }
+            if (capn < (uint64_t)c.trim[i] + c.keep[i])
+                return err.set(RC_SOFT, "chain %u capacity %llu < trim %u + keep %u", i,
+                               (unsigned long long)capn, c.trim[i], c.keep[i]);
+            P.first.push_back(c.first[i] + (uint32_t)pkt_base);
+            P.npkts.push_back(c.npkts[i]);
+            P.chans.push_back((uint8_t)d.channels);
+            P.trim.push_back(c.trim[i]);
+            P.keep.push_back(c.keep[i]);
+            P.out_off.push_back(P.out_elems + fkeep * d.channels);
+            P.cap.push_back(capn);
+            fkeep += c.keep[i];
+        }
+        P.file_keep.push_back(fkeep);
+        P.file_chans.push_back(d.channels);
+        P.file_play48.push_back(d.play48);
+        P.out_elems += fkeep * d.channels;
+    }
+    return RC_OK;
+}
+
+// H2D of a plan, one decode launch into G.pcm, D2H of the results, validation.
+int run_plan(const Plan &P, cudaStream_t st, Err &err)
+{
+    int rc;
+    uint32_t nch = (uint32_t)P.first.size();
+    auto r16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    size_t tbl = r16(P.blob.size()) + r16(8ull * P.off.size()) + r16(4ull * P.len.size()) + 2 * r16(4ull * nch) +
+                 r16(nch) + 3 * r16(8ull * nch);
+    if ((rc = pin_grow(G.hpin, tbl, err))) return rc;
+    if ((rc = gpu_grow(G.data, P.blob.size() + 16, err))) return rc;
+    if ((rc = gpu_grow(G.off, 8ull * P.off.size(), err))) return rc;
+    if ((rc = gpu_grow(G.len, 4ull * P.len.size(), err))) return rc;
+    if ((rc = gpu_grow(G.first, 4ull * nch, err))) return rc;
+    if ((rc = gpu_grow(G.npkts, 4ull * nch, err))) return rc;
+    if ((rc = gpu_grow(G.chans, nch, err))) return rc;
+    if ((rc = gpu_grow(G.trim, 8ull * nch, err))) return rc;
+    if ((rc = gpu_grow(G.keep, 8ull * nch, err))) return rc;
+    if ((rc = gpu_grow(G.out_off, 8ull * nch, err))) return rc;
+    if ((rc = gpu_grow(G.res, 16ull * nch, err))) return rc;
+    if ((rc = gpu_grow(G.pcm, 2ull * P.out_elems + 16, err))) return rc;
+    // stage everything through one pinned buffer, then one async copy per table
+    uint8_t *h = (uint8_t *)G.hpin.p;
+    size_t o = 0;
+    auto stage = [&](Grow &dst, const void *src, size_t bytes) -> int {
+        if (!bytes) return RC_OK;
+        memcpy(h + o, src, bytes);
+        cudaError_t e = cudaMemcpyAsync(dst.p, h + o, bytes, cudaMemcpyHostToDevice, st);
+        o += (bytes + 15) & ~(size_t)15;
+        if (e != cudaSuccess) return err.set(RC_CUDA, "cudaMemcpyAsync: %s", cudaGetErrorString(e));
+        return RC_OK;
+    };
+    if ((rc = stage(G.data, P.blob.data(), P.blob.size()))) return rc;
+    if ((rc = stage(G.off, P.off.data(), 8ull * P.off.size()))) return rc;
+    if ((rc = stage(G.len, P.len.data(), 4ull * P.len.size()))) return rc;
+    if ((rc = stage(G.first, P.first.data(), 4ull * nch))) return rc;
+    if ((rc = stage(G.npkts, P.npkts.data(), 4ull * nch))) return rc;
+    if ((rc = stage(G.chans, P.chans.data(), nch))) return rc;
+    if ((rc = stage(G.trim, P.trim.data(), 8ull * nch))) return rc;
+    if ((rc = stage(G.keep, P.keep.data(), 8ull * nch))) return rc;
+    if ((rc = stage(G.out_off, P.out_off.data(), 8ull * nch))) return rc;
+    cuopus_batch b;
+    memset(&b, 0, sizeof b);
+    b.data = (const uint8_t *)G.data.p;
+    b.off = (const uint64_t *)G.off.p;
+    b.len = (const uint32_t *)G.len.p;
+    b.first = (const uint32_t *)G.first.p;
+    b.npkts = (const uint32_t *)G.npkts.p;
+    b.channels = (const uint8_t *)G.chans.p;
+    b.trim = (const uint64_t *)G.trim.p;
+    b.keep = (const uint64_t *)G.keep.p;
+    b.out_off = (const uint64_t *)G.out_off.p;
+    b.out = (int16_t *)G.pcm.p;
+    b.res = (uint32_t *)G.res.p;
+    b.nchains = (int32_t)nch;
+    b.width = default_width();
+    // longest chains first through the device queue: packets are the proxy
+    std::vector<uint32_t> order(nch);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t x, uint32_t y) { return P.cap[x] * P.chans[x] > P.cap[y] * P.chans[y]; });
+    b.schedule = 1;
+    b.order = order.data();
+    float kms = 0.f;
+    if ((rc = decode_batch(&b, st, &kms, err))) return rc;
+    return RC_OK;
+}
+
+int validate(const Plan &P, cudaStream_t st, Err &err)
+{
+    uint32_t nch = (uint32_t)P.first.size();
+    std::vector<uint32_t> res(4ull * nch);
+    CK(cudaMemcpyAsync(res.data(), G.res.p, 16ull * nch, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (uint32_t c = 0; c < nch; c++) {
+        int32_t stop = (int32_t)res[4 * c];
+        uint32_t samples = res[4 * c + 1];
+        if (stop != 0) return err.set(RC_SOFT, "chain %u: device decode error %d", c, stop);
+        if (samples != P.cap[c])
+            return err.set(RC_SOFT, "chain %u: decoded %u samples, expected %llu", c, samples,
+                           (unsigned long long)P.cap[c]);
+    }
+    return RC_OK;
+}
+
+int64_t out16_of(int64_t play48)
+{
+    int64_t v = (int64_t)((play48 - (int64_t)SWR_TAIL_48K) / 3);
+    return v < 0 ? 0 : v;
+}
+
+int resample(const int16_t *in, int64_t avail, int64_t n_out, float *out, cudaStream_t st, Err &err)
+{
+    if (n_out <= 0) return RC_OK;
+    int rc = ensure_taps(st, err);
+    if (rc) return rc;
+    long long blocks = (n_out + cuo::RS_TILE_OUT - 1) / cuo::RS_TILE_OUT;
+    if (blocks > 0x7fffffffLL) return err.set(RC_ARG, "resample length too large");
+    cuo::k_resample48to16<<<(unsigned)blocks, cuo::RS_THREADS, 0, st>>>(in, avail, n_out, out);
+    CK(cudaGetLastError());
+    return RC_OK;
+}
+
+int f16k_impl(const uint8_t *const *oggs, const size_t *ns, int nfiles, float *const *out_devs,
+              const size_t *out_caps, int64_t *out_lens, cudaStream_t st, bool enforce_max_batch, Err &err)
+{
+    G.last_ovf = 0;
+    if (out_lens) for (int f = 0; f < nfiles; f++) out_lens[f] = 0;
+    if (nfiles <= 0) return RC_OK;
+    int rc = refuse_capture(st, err);
+    if (rc) return rc;
+    Plan P;
+    if ((rc = plan_files(oggs, ns, nfiles, true, P, err))) return rc;
+    if (P.first.empty()) return err.set(RC_SOFT, "no chains");
+    if (enforce_max_batch) {
+        int max_batch = env_i("CUOPUS_MAX_BATCH", 2048);
+        if ((int)P.first.size() > max_batch)
+            return err.set(RC_ARG, "merged chains %zu > max_batch %d (decode files individually)", P.first.size(),
+                           max_batch);
+    }
+    std::vector<int64_t> n16(nfiles);
+    for (int f = 0; f < nfiles; f++) {
+        n16[f] = out16_of((int64_t)P.file_keep[f]);   // sum(keep) == playable samples
+        if (!out_caps || (uint64_t)n16[f] > out_caps[f])
+            return err.set(RC_ARG, "file %d: output capacity %zu < required %lld", f, out_caps ? out_caps[f] : 0,
+                           (long long)n16[f]);
+        if (n16[f] > 0 && (!out_devs || !out_devs[f])) return err.set(RC_ARG, "file %d: out_dev is NULL", f);
+    }
+    int64_t total16 = 0;
+    for (int f = 0; f < nfiles; f++) total16 += n16[f];
+    if (total16 == 0) return RC_OK;
+    if ((rc = run_plan(P, st, err))) return rc;
+    for (int f = 0; f < nfiles; f++) {
+        const int16_t *in = (const int16_t *)G.pcm.p + P.file_out0[f];
+        if ((rc = resample(in, (int64_t)P.file_keep[f], n16[f], out_devs[f], st, err))) return rc;
+    }
+    if ((rc = validate(P, st, err))) return rc;
+    if (out_lens) for (int f = 0; f < nfiles; f++) out_lens[f] = n16[f];
+    return RC_OK;
+}
+
+} // namespace
+
+// ====================================================================== C ABI
+
+extern "C" int cuopus_last_arena_overflow(void) { return G.last_ovf; }
+
+extern "C" long long cuopus_workspace_bytes(void) { return G.dev_bytes; }
+
+extern "C" void cuopus_release_workspaces(void)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    Grow *all[] = {&G.data, &G.off, &G.len, &G.first, &G.npkts, &G.chans, &G.trim, &G.keep,
+                   &G.out_off, &G.order, &G.res, &G.slots, &G.queue, &G.pcm};
+    for (Grow *g : all) {
+        if (g->p) cudaFree(g->p);
+        g->p = nullptr;
+        g->cap = 0;
+    }
+    if (G.hpin.p) cudaFreeHost(G.hpin.p);
+    G.hpin.p = nullptr;
+    G.hpin.cap = 0;
+    G.dev_bytes = 0;
+    G.taps_dev = -1;
+}
+
+extern "C" int cuopus_probe(const uint8_t *ogg, size_t n, int64_t *samples16k, char *errbuf, size_t errcap)
+{
+    Err err(errbuf, errcap);
+    if (!samples16k) return err.set(RC_ARG, "samples16k is NULL");
+    if (!ogg || !n) return err.set(RC_ARG, "empty input");
+    cuo_host::Demux d;
+    std::string e;
+    if (!cuo_host::demux_and_chain(ogg, n, 1.0, 250.0, true, d, nullptr, e)) return err.set(RC_SOFT, "%s", e.c_str());
+    *samples16k = out16_of(d.play48);
+    return RC_OK;
+}
+
+extern "C" int cuopus_probe_pcm(const uint8_t *ogg, size_t n, int64_t *play48, int32_t *channels, char *errbuf,
+                                size_t errcap)
+{
+    Err err(errbuf, errcap);
+    if (!play48) return err.set(RC_ARG, "play48 is NULL");
+    if (!ogg || !n) return err.set(RC_ARG, "empty input");
+    cuo_host::Demux d;
+    std::string e;
+    if (!cuo_host::demux_and_chain(ogg, n, 1.0, 250.0, false, d, nullptr, e)) return err.set(RC_SOFT, "%s", e.c_str());
+    *play48 = d.play48 > 0 ? d.play48 : 0;
+    if (channels) *channels = d.channels;
+    return RC_OK;
+}
+
+extern "C" int cuopus_index(const uint8_t *ogg, size_t n, double seg_s, double preroll_ms, int require_mono,
+                            int64_t *n_packets, int64_t *n_chains, int64_t *blob_bytes, int32_t *channels,
+                            int64_t *play48, uint8_t *blob, uint64_t *pkt_off, uint32_t *pkt_len, uint32_t *first,
+                            uint32_t *npkts, uint32_t *trim, uint32_t *keep, char *errbuf, size_t errcap)
+{
+    Err err(errbuf, errcap);
+    if (!ogg || !n) return err.set(RC_ARG, "empty input");
+    cuo_host::Demux d;
+    cuo_host::Chains c;
+    std::string e;
+    if (!cuo_host::demux_and_chain(ogg, n, seg_s, preroll_ms, require_mono != 0, d, &c, e))
+        return err.set(RC_SOFT, "%s", e.c_str());
+    if (n_packets) *n_packets = d.n_packets();
+    if (n_chains) *n_chains = c.size();
+    if (blob_bytes) *blob_bytes = (int64_t)d.blob.size();
+    if (channels) *channels = d.channels;
+    if (play48) *play48 = d.play48;
+    if (!blob) return RC_OK;
+    if (!pkt_off || !pkt_len || !first || !npkts || !trim || !keep) return err.set(RC_ARG, "NULL output array");
+    memcpy(blob, d.blob.data(), d.blob.size());
+    memcpy(pkt_off, d.off.data(), 8 * d.off.size());
+    memcpy(pkt_len, d.len.data(), 4 * d.len.size());
+    memcpy(first, c.first.data(), 4 * c.size());
+    memcpy(npkts, c.npkts.data(), 4 * c.size());
+    memcpy(trim, c.trim.data(), 4 * c.size());
+    memcpy(keep, c.keep.data(), 4 * c.size());
+    return RC_OK;
+}
+
+extern "C" int cuopus_decode_f16k_on(const uint8_t *ogg, size_t n, float *out_dev, size_t out_cap, int64_t *out_len,
+                                     void *cuda_stream, char *errbuf, size_t errcap)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    Err err(errbuf, errcap);
+    const uint8_t *oggs[1] = {ogg};
+    size_t ns[1] = {n};
+    float *outs[1] = {out_dev};
+    size_t caps[1] = {out_cap};
+    if (!ogg || !n) return err.set(RC_ARG, "empty input");
+    return f16k_impl(oggs, ns, 1, outs, caps, out_len, (cudaStream_t)cuda_stream, false, err);
+}
+
+extern "C" int cuopus_decode_f16k(const uint8_t *ogg, size_t n, float *out_dev, size_t out_cap, int64_t *out_len,
+                                  char *errbuf, size_t errcap)
+{
+    return cuopus_decode_f16k_on(ogg, n, out_dev, out_cap, out_len, nullptr, errbuf, errcap);
+}
+
+extern "C" int cuopus_decode_f16k_multi(const uint8_t *const *oggs, const size_t *ns, int nfiles,
+                                        float *const *out_devs, const size_t *out_caps, int64_t *out_lens,
+                                        void *cuda_stream, char *errbuf, size_t errcap)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    Err err(errbuf, errcap);
+    return f16k_impl(oggs, ns, nfiles, out_devs, out_caps, out_lens, (cudaStream_t)cuda_stream, nfiles > 1, err);
+}
+
+extern "C" int cuopus_decode_i16_multi(const uint8_t *const *oggs, const size_t *ns, int nfiles,
+                                       int16_t *const *out_devs, const size_t *out_caps, int64_t *out_lens,
+                                       int32_t *out_channels, void *cuda_stream, char *errbuf, size_t errcap)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    Err err(errbuf, errcap);
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    if (out_lens) for (int f = 0; f < nfiles; f++) out_lens[f] = 0;
+    if (nfiles <= 0) return RC_OK;
+    int rc = refuse_capture(st, err);
+    if (rc) return rc;
+    Plan P;
+    if ((rc = plan_files(oggs, ns, nfiles, false, P, err))) return rc;
+    if (P.first.empty()) return err.set(RC_SOFT, "no chains");
+    for (int f = 0; f < nfiles; f++) {
+        uint64_t need = P.file_keep[f] * (uint64_t)P.file_chans[f];
+        if (!out_caps || need > out_caps[f])
+            return err.set(RC_ARG, "file %d: output capacity %zu < required %llu", f, out_caps ? out_caps[f] : 0,
+                           (unsigned long long)need);
+        if (need && (!out_devs || !out_devs[f])) return err.set(RC_ARG, "file %d: out_dev is NULL", f);
+    }
+    if ((rc = run_plan(P, st, err))) return rc;
+    for (int f = 0; f < nfiles; f++) {
+        uint64_t need = P.file_keep[f] * (uint64_t)P.file_chans[f];
+        if (need)
+            CK(cudaMemcpyAsync(out_devs[f], (const int16_t *)G.pcm.p + P.file_out0[f], 2 * need,
+                               cudaMemcpyDeviceToDevice, st));
+    }
+    if ((rc = validate(P, st, err))) return rc;
+    for (int f = 0; f < nfiles; f++) {
+        if (out_lens) out_lens[f] = (int64_t)P.file_keep[f];
+        if (out_channels) out_channels[f] = P.file_chans[f];
+    }
+    return RC_OK;
+}
+
+extern "C" int cuopus_decode_batch(const cuopus_batch *b, void *cuda_stream, float *kernel_ms, char *errbuf,
+                                   size_t errcap)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    Err err(errbuf, errcap);
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    int rc = refuse_capture(st, err);
+    if (rc) return rc;
+    if ((rc = decode_batch(b, st, kernel_ms, err))) return rc;
+    CK(cudaStreamSynchronize(st));
+    return RC_OK;
+}
+
+extern "C" int cuopus_resample48to16(const int16_t *in_dev, int64_t avail, int64_t n_out, float *out_dev,
+                                     void *cuda_stream, char *errbuf, size_t errcap)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    Err err(errbuf, errcap);
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    int rc = refuse_capture(st, err);
+    if (rc) return rc;
+    if (n_out > 0 && (!in_dev || !out_dev)) return err.set(RC_ARG, "NULL buffer");
+    if ((rc = resample(in_dev, avail, n_out, out_dev, st, err))) return rc;
+    CK(cudaStreamSynchronize(st));
+    return RC_OK;
+}
+
+extern "C" int cuopus_warmup(char *errbuf, size_t errcap)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    Err err(errbuf, errcap);
+    int rc = ensure_occupancy(err);
+    if (rc) return rc;
+    if ((rc = ensure_events(err))) return rc;
+    int width = default_width();
+    long long nslots = (long long)G.sm_count * G.occ_blocks * (BLOCK / width);
+    if ((rc = gpu_grow(G.slots, (size_t)nslots * sizeof(cuo::ChainSlot), err))) return rc;
+    if ((rc = ensure_taps(nullptr, err))) return rc;
+    CK(cudaDeviceSynchronize());
+    return RC_OK;
+}
+
+extern "C" long long cuopus_slot_bytes(void) { return (long long)sizeof(cuo::ChainSlot); }
+
+extern "C" int cuopus_default_width(void) { return default_width(); }

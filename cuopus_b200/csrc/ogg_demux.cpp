@@ -1,0 +1,244 @@
+// Host-side Ogg-Opus demuxer and chain builder (see ogg_demux.h).
+#include "ogg_demux.h"
+
+#include <string.h>
+
+#include <algorithm>
+#include <cstdio>
+
+namespace cuo_host {
+
+int toc_samples48(const uint8_t *p, uint32_t len)
+{
+    // frame duration in quarter milliseconds per TOC configuration
+    static const int qms[32] = {40, 80, 160, 240, 40, 80, 160, 240, 40, 80, 160, 240, 40, 80, 40, 80,
+                                10, 20, 40, 80, 10, 20, 40, 80, 10, 20, 40, 80, 10, 20, 40, 80};
+    if (!len) return 0;
+    int code = p[0] & 3, nf;
+    if (code == 0) nf = 1;
+    else if (code < 3) nf = 2;
+    else {
+        if (len < 2) return 0;
+        nf = p[1] & 0x3F;
+    }
+    return qms[p[0] >> 3] * 12 * nf;
+}
+
+namespace {
+
+struct Span {
+    uint64_t start;
+    uint32_t len;
+    uint32_t page;
+    bool done;
+};
+
+int64_t rd_i64le(const uint8_t *p)
+{
+    uint64_t v = 0;
+    for (int i = 7; i >= 0; i--) v = (v << 8) | p[i];
+    return (int64_t)v;
+}
+
+std::string fmt(const char *f, long long a = 0, long long b = 0, long long c = 0, long long d = 0)
+{
+    char buf[256];
+    snprintf(buf, sizeof buf, f, a, b, c, d);
+    return buf;
+}
+
+} // namespace
+
+bool demux(const uint8_t *data, size_t n, Demux &d, std::string &err)
+{
+    d = Demux();
+    if (!data || n == 0) { err = "empty stream"; return false; }
+    std::vector<Span> spans;
+    std::vector<int64_t> page_granule;
+    size_t pos = 0;
+    static const uint8_t magic[4] = {'O', 'g', 'g', 'S'};
+    while (pos < n) {
+        const uint8_t *hit = std::search(data + pos, data + n, magic, magic + 4);
+        if (hit == data + n) break;
+        size_t idx = (size_t)(hit - data);
+        if (idx + 27 > n) break;
+        int64_t granule = rd_i64le(data + idx + 6);
+        uint32_t nseg = data[idx + 26];
+        const uint8_t *table = data + idx + 27;
+        uint64_t body = idx + 27 + nseg;
+        if (body > n) break;
+        uint64_t blen = 0;
+        for (uint32_t i = 0; i < nseg; i++) blen += table[i];
+        if (body + blen > n) break;
+        uint32_t pg = (uint32_t)page_granule.size();
+        page_granule.push_back(granule);
+        uint64_t run_start = body;
+        uint32_t run_len = 0;
+        int last = 0;
+        for (uint32_t i = 0; i < nseg; i++) {
+            run_len += table[i];
+            last = table[i];
+            if (table[i] < 255) {
+                spans.push_back({run_start, run_len, pg, true});
+                run_start += run_len;
+                run_len = 0;
+            }
+        }
+        if (run_len > 0 || (nseg > 0 && last == 255)) spans.push_back({run_start, run_len, pg, false});
+        pos = body + blen;
+    }
+    if (page_granule.empty()) { err = "no OGG pages found"; return false; }
+    d.n_pages = (uint32_t)page_granule.size();
+
+    // reassemble packets
+    std::vector<uint64_t> pkt_span_first;
+    std::vector<uint32_t> pkt_len, pkt_page;
+    {
+        uint64_t acc = 0;
+        size_t first_span = 0;
+        for (size_t i = 0; i < spans.size(); i++) {
+            if (i == 0 || spans[i - 1].done) first_span = i;
+            acc += spans[i].len;
+            if (spans[i].done) {
+                pkt_span_first.push_back(first_span);
+                pkt_len.push_back((uint32_t)acc);
+                pkt_page.push_back(spans[i].page);
+                acc = 0;
+            }
+        }
+    }
+    size_t npk = pkt_len.size();
+    if (npk < 2) { err = "not an OGG Opus stream (fewer than 2 packets)"; return false; }
+    const Span &h = spans[pkt_span_first[0]];
+    // OpusHead fields are read from the first span, as the reference does
+    if (pkt_len[0] < 19 || h.len < 12 || memcmp(data + h.start, "OpusHead", 8) != 0) {
+        err = "not an OGG Opus stream (no OpusHead)";
+        return false;
+    }
+    d.channels = data[h.start + 9];
+    d.preskip = data[h.start + 10] | (data[h.start + 11] << 8);
+
+    size_t n_audio = npk - 2;
+    uint64_t audio_bytes = 0;
+    for (size_t i = 2; i < npk; i++) audio_bytes += pkt_len[i];
+    if (audio_bytes > 0xFFFFFFFFull) { err = "stream too large"; return false; }
+    d.blob.resize(audio_bytes);
+    d.off.resize(n_audio);
+    d.len.resize(n_audio);
+    d.sample_off.resize(n_audio);
+    std::vector<uint32_t> apage(n_audio);
+    uint64_t w = 0;
+    for (size_t k = 0; k < n_audio; k++) {
+        size_t pi = k + 2;
+        d.off[k] = w;
+        d.len[k] = pkt_len[pi];
+        apage[k] = pkt_page[pi];
+        // copy the spans of this packet
+        size_t s = pkt_span_first[pi];
+        uint32_t remaining = pkt_len[pi];
+        while (remaining > 0 || !spans[s].done) {
+            memcpy(d.blob.data() + w, data + spans[s].start, spans[s].len);
+            w += spans[s].len;
+            remaining -= spans[s].len;
+            if (spans[s].done) break;
+            s++;
+        }
+    }
+    if (w != audio_bytes) { err = "internal: blob size mismatch"; return false; }
+
+    // TOC offsets and granule cross-check
+    int64_t cum = 0;
+    for (size_t k = 0; k < n_audio; k++) {
+        d.sample_off[k] = cum;
+        cum += toc_samples48(d.blob.data() + d.off[k], d.len[k]);
+    }
+    d.toc_total = cum;
+    std::vector<int64_t> page_end(page_granule.size(), -1);
+    int64_t final_page = -1;
+    for (size_t k = 0; k < n_audio; k++) {
+        uint32_t pg = apage[k];
+        page_end[pg] = d.sample_off[k] + toc_samples48(d.blob.data() + d.off[k], d.len[k]);
+        if ((int64_t)pg > final_page) final_page = pg;
+    }
+    int last_dur = n_audio ? toc_samples48(d.blob.data() + d.off[n_audio - 1], d.len[n_audio - 1]) : 0;
+    int64_t last_granule = 0;
+    for (size_t pg = 0; pg < page_granule.size(); pg++) {
+        int64_t g = page_granule[pg];
+        if (g != -1 && g > last_granule) last_granule = g;
+        if (g == -1 || page_end[pg] < 0) continue;
+        d.granule_checked++;
+        if (g == page_end[pg]) d.granule_match++;
+        else if ((int64_t)pg == final_page && page_end[pg] - g >= 0 && page_end[pg] - g < last_dur)
+            d.granule_match++;
+    }
+    d.last_granule = last_granule;
+    d.end_trim = d.toc_total - last_granule;
+    d.play48 = last_granule - d.preskip;
+    return true;
+}
+
+bool build_chains(const Demux &d, double seconds, double preroll_ms, Chains &c, std::string &err)
+{
+    c = Chains();
+    int64_t step = (int64_t)(seconds * 48000);
+    int64_t preroll = (int64_t)(preroll_ms * 48);
+    int64_t total = d.play48;
+    uint32_t npk = d.n_packets();
+    if (total <= 0) { err = "no playable samples"; return false; }
+    if (step <= 0) { err = "bad segment length"; return false; }
+    std::vector<int64_t> cum(npk + 1, 0);
+    for (uint32_t k = 0; k < npk; k++)
+        cum[k + 1] = cum[k] + toc_samples48(d.blob.data() + d.off[k], d.len[k]);
+    const std::vector<int64_t> &so = d.sample_off;
+    int64_t kept = 0;
+    for (int64_t k = 0; k * step < total; k++) {
+        int64_t ps = k * step, pe = std::min((k + 1) * step, total);
+        int64_t ts = ps + d.preskip, te = pe + d.preskip;
+        int64_t target = std::max<int64_t>(0, ts - preroll);
+        int64_t first = (int64_t)(std::upper_bound(so.begin(), so.end(), target) - so.begin()) - 1;
+        if (first < 0) first = 0;
+        if (cum[first + 1] <= target) first++;
+        int64_t last = (int64_t)(std::lower_bound(so.begin(), so.end(), te) - so.begin()) - 1;
+        if (last < first) last = first;
+        if (first >= (int64_t)npk || last >= (int64_t)npk) {
+            err = fmt("chain %lld: packet range beyond the stream", k);
+            return false;
+        }
+        int64_t trim = ts - so[first], keep = pe - ps;
+        if (trim < 0) { err = fmt("chain %lld: negative trim %lld", k, trim); return false; }
+        int64_t capn = cum[last + 1] - cum[first];
+        if (capn < trim + keep) {
+            err = fmt("chain %lld: capacity %lld < trim %lld + keep %lld", k, capn, trim, keep);
+            return false;
+        }
+        c.first.push_back((uint32_t)first);
+        c.npkts.push_back((uint32_t)(last - first + 1));
+        c.trim.push_back((uint32_t)trim);
+        c.keep.push_back((uint32_t)keep);
+        kept += keep;
+    }
+    if (kept != total) { err = fmt("internal: sum(keep) %lld != playable %lld", kept, total); return false; }
+    return true;
+}
+
+bool demux_and_chain(const uint8_t *data, size_t n, double seconds, double preroll_ms, bool require_mono,
+                     Demux &d, Chains *c, std::string &err)
+{
+    if (!demux(data, n, d, err)) return false;
+    if (require_mono && d.channels != 1) {
+        err = fmt("only mono supported (channels=%lld)", d.channels);
+        return false;
+    }
+    if (d.channels != 1 && d.channels != 2) {
+        err = fmt("unsupported channel count %lld", d.channels);
+        return false;
+    }
+    if (d.granule_match != d.granule_checked) {
+        err = fmt("granule cross-check failed (%lld/%lld)", d.granule_match, d.granule_checked);
+        return false;
+    }
+    if (c && !build_chains(d, seconds, preroll_ms, *c, err)) return false;
+    return true;
+}
+
+} // namespace cuo_host

@@ -1,0 +1,59 @@
+// Host-side Ogg-Opus demuxer and chain builder.
+//
+// Behaviour of the reference's cu_demux_mem / cu_build_chains2
+// (cuopus_demux.h:79-269, :293-378; Python twin ogg_index.py:75-209, :319-367):
+//   * every "OggS" page is parsed (CRC not checked); lacing runs < 255 end a
+//     packet, a trailing run continues on the next page; a partial packet at
+//     end of file is dropped;
+//   * packet 0 must be OpusHead (>= 19 bytes): channels = byte 9, pre-skip =
+//     bytes 10-11; packets 0 and 1 (OpusTags) are headers;
+//   * each audio packet's 48 kHz duration comes from its TOC (RFC 6716 3.1);
+//   * every page with a granule and a completed packet is cross-checked
+//     against the cumulative TOC sum; the final data page may be short by less
+//     than the last packet's duration (RFC 7845 end trim);
+//   * playable samples = last granule - pre-skip;
+//   * chains: the playable range is cut every `seconds`; each chain starts
+//     `preroll_ms` early (clamped at 0), `trim` drops preroll + pre-skip and
+//     `keep` is exact, so sum(keep) == playable.
+// The implementation is std::vector based and allocation-checked; errors are
+// returned as a message, never by exiting.
+#pragma once
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+namespace cuo_host {
+
+int toc_samples48(const uint8_t *p, uint32_t len);
+
+struct Demux {
+    std::vector<uint8_t> blob;        // audio packets back to back
+    std::vector<uint64_t> off;        // per packet offset into blob
+    std::vector<uint32_t> len;        // per packet length
+    std::vector<int64_t> sample_off;  // per packet cumulative 48 kHz offset
+    int channels = 0;
+    int preskip = 0;
+    int64_t toc_total = 0;
+    int64_t last_granule = 0;
+    int64_t play48 = 0;               // last_granule - preskip
+    int64_t end_trim = 0;
+    uint32_t n_pages = 0;
+    uint32_t granule_checked = 0, granule_match = 0;
+    uint32_t n_packets() const { return (uint32_t)len.size(); }
+};
+
+struct Chains {
+    std::vector<uint32_t> first, npkts, trim, keep;
+    uint32_t size() const { return (uint32_t)first.size(); }
+};
+
+// Returns true on success; on failure `err` holds the reason.
+bool demux(const uint8_t *data, size_t n, Demux &d, std::string &err);
+bool build_chains(const Demux &d, double seconds, double preroll_ms, Chains &c, std::string &err);
+
+// Demux + the reference's acceptance checks (granule cross-check; mono only
+// when require_mono) + chain table.
+bool demux_and_chain(const uint8_t *data, size_t n, double seconds, double preroll_ms, bool require_mono,
+                     Demux &d, Chains *c, std::string &err);
+
+} // namespace cuo_host

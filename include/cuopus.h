@@ -1,0 +1,140 @@
+/* libcuopus — batched Opus decode on NVIDIA Blackwell (sm_100a).
+ *
+ * C ABI of the drop-in library.  The first eight entry points have exactly the
+ * signatures and semantics of the reference's libcuopus.cu (cited per entry);
+ * the rest extend it and say so.
+ *
+ * Return codes (reference libcuopus.cu:48-51): 0 ok; 1 soft failure (bad
+ * stream or decode validation; the CUDA context is healthy, the caller may
+ * fall back to a CPU decoder); 2 CUDA error (context suspect); 3 caller error
+ * (capacity, NULL pointer, stream capture in progress, too many merged
+ * chains).  errbuf, when not NULL, always receives a NUL-terminated message.
+ *
+ * Threading: the library never creates a context, thread or stream; all work
+ * is issued on the caller's stream (or stream 0) of the current device, and
+ * every call synchronises that stream before it returns.  It refuses to run
+ * while that stream is capturing a CUDA graph.  Workspaces are process-global
+ * and grow-only; calls must not run concurrently from several host threads.
+ */
+#ifndef CUOPUS_H
+#define CUOPUS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Demux + validate (mono, granule cross-check) and return the exact f16k
+ * output length max(0, (playable48 - 48) / 3).  Host only.
+ * Replaces reference libcuopus.cu:223-236 (cuopus_probe). */
+int cuopus_probe(const uint8_t *ogg, size_t n, int64_t *samples16k, char *errbuf, size_t errcap);
+
+/* cuopus_decode_f16k_on on stream 0.  Replaces libcuopus.cu:462-468. */
+int cuopus_decode_f16k(const uint8_t *ogg, size_t n, float *out_dev, size_t out_cap, int64_t *out_len,
+                       char *errbuf, size_t errcap);
+
+/* Decode a mono Ogg Opus stream cut into CUOPUS_SEG_S chains (default 1 s)
+ * with CUOPUS_PREROLL_MS preroll (default 250 ms) and resample 48->16 kHz into
+ * out_dev (float32, out_cap samples) on cuda_stream.  Replaces
+ * libcuopus.cu:238-460 (cuopus_decode_f16k_on). */
+int cuopus_decode_f16k_on(const uint8_t *ogg, size_t n, float *out_dev, size_t out_cap, int64_t *out_len,
+                          void *cuda_stream, char *errbuf, size_t errcap);
+
+/* N files in one decode launch; per-file output identical to the single-file
+ * call.  RC 3 when the merged chain count exceeds CUOPUS_MAX_BATCH.
+ * Replaces libcuopus.cu:482-741 (cuopus_decode_f16k_multi). */
+int cuopus_decode_f16k_multi(const uint8_t *const *oggs, const size_t *ns, int nfiles, float *const *out_devs,
+                             const size_t *out_caps, int64_t *out_lens, void *cuda_stream, char *errbuf,
+                             size_t errcap);
+
+/* Pre-size the decoder slots and upload the resampler taps on the current
+ * device so the first decode pays only for the decode.  Replaces
+ * libcuopus.cu:746-776 (cuopus_warmup). */
+int cuopus_warmup(char *errbuf, size_t errcap);
+
+/* 1 if the last call failed on decoder scratch overflow.  This decoder sizes
+ * all scratch statically per slot, so it always returns 0.  Replaces
+ * libcuopus.cu:201. */
+int cuopus_last_arena_overflow(void);
+
+/* Bytes held in grow-only device workspaces.  Replaces libcuopus.cu:203. */
+long long cuopus_workspace_bytes(void);
+
+/* Free every workspace.  Replaces libcuopus.cu:205-221. */
+void cuopus_release_workspaces(void);
+
+/* ------------------------------------------------------------------ extensions */
+
+/* Extension (the reference CLI's int16 "DECODE" output, for mono and stereo):
+ * decode N files to 48 kHz interleaved int16 playable PCM.  out_caps are in
+ * int16 elements; out_lens receive samples per channel; out_channels (may be
+ * NULL) the channel count.  Chains as in cuopus_decode_f16k_on. */
+int cuopus_decode_i16_multi(const uint8_t *const *oggs, const size_t *ns, int nfiles, int16_t *const *out_devs,
+                            const size_t *out_caps, int64_t *out_lens, int32_t *out_channels, void *cuda_stream,
+                            char *errbuf, size_t errcap);
+
+/* Extension: device-resident batch decode, the engine under every entry
+ * above.  All pointers are device pointers unless noted.  Chains are decoded
+ * by groups of `width` lanes; `schedule` 0 = static (chain c on group
+ * c mod groups), 1 = device work queue in `order` (host pointer or NULL =
+ * identity).  `max_groups` bounds the resident groups (0 = fill the GPU).
+ * pkt_nsamp / pkt_rng (device, may be NULL) receive per-packet sample counts
+ * and final ranges at rec_off[c] + k.  res: 4 x uint32 per chain
+ * {stop, samples, final_range, cycles}.  kernel_ms (host, may be NULL)
+ * receives the decode kernel time measured with events on the stream. */
+typedef struct cuopus_batch {
+    const uint8_t *data;
+    const uint64_t *off;
+    const uint32_t *len;
+    const uint32_t *first;
+    const uint32_t *npkts;
+    const uint8_t *channels;
+    const uint64_t *trim;
+    const uint64_t *keep;
+    const uint64_t *out_off;
+    int16_t *out;
+    const uint64_t *rec_off;
+    uint32_t *pkt_nsamp;
+    uint32_t *pkt_rng;
+    uint32_t *res;
+    int32_t nchains;
+    int32_t width;
+    int32_t schedule;
+    int32_t max_groups;
+    const uint32_t *order;
+} cuopus_batch;
+
+int cuopus_decode_batch(const cuopus_batch *b, void *cuda_stream, float *kernel_ms, char *errbuf, size_t errcap);
+
+/* Extension: fp32 48->16 kHz resample of a device int16 mono stream (the
+ * kernel behind the f16k entries): out[i], i < n_out, from in[0..avail). */
+int cuopus_resample48to16(const int16_t *in_dev, int64_t avail, int64_t n_out, float *out_dev, void *cuda_stream,
+                          char *errbuf, size_t errcap);
+
+/* Extension (host only, mono or stereo): demux + validate; play48 receives
+ * the playable samples per channel at 48 kHz and channels the channel count. */
+int cuopus_probe_pcm(const uint8_t *ogg, size_t n, int64_t *play48, int32_t *channels, char *errbuf,
+                     size_t errcap);
+
+/* Extension: the host demuxer and chain builder (the reference CLI's
+ * --dump-blob / --dump-chains data, cuopus_demux.h:79-378).  Two calls: with
+ * blob == NULL only the counts are returned; then pass arrays of those sizes.
+ * seg_s / preroll_ms choose the chains (1.0 / 250.0 in the entry points above);
+ * require_mono applies the f16k entry points' mono check. */
+int cuopus_index(const uint8_t *ogg, size_t n, double seg_s, double preroll_ms, int require_mono,
+                 int64_t *n_packets, int64_t *n_chains, int64_t *blob_bytes, int32_t *channels, int64_t *play48,
+                 uint8_t *blob, uint64_t *pkt_off, uint32_t *pkt_len, uint32_t *first, uint32_t *npkts,
+                 uint32_t *trim, uint32_t *keep, char *errbuf, size_t errcap);
+
+/* Extension: bytes of device state per decoder slot, and the number of lanes
+ * per chain the entry points use (CUOPUS_STRIDE, default 32). */
+long long cuopus_slot_bytes(void);
+int cuopus_default_width(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUOPUS_H */
