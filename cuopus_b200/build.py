@@ -52,15 +52,23 @@ def _run(cmd):
 
 
 def build_libcuopus(force=False):
-    deps = _sources("libcuopus.cu", "kernels.cuh", "ogg_demux.cpp", "ogg_demux.h", "dec") + \
+    deps = _sources("libcuopus.cu", "decode_kernel.cu", "kernels.cuh", "ogg_demux.cpp", "ogg_demux.h", "dec") + \
         [os.path.join(ROOT, "include", "cuopus.h")]
     if not force and not _stale(LIBCUOPUS, deps):
         return LIBCUOPUS
     os.makedirs(LIB, exist_ok=True)
+    obj = os.path.join(LIB, "obj")
+    os.makedirs(obj, exist_ok=True)
+    common = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-I", CSRC]
+    # The decoder kernel is built at ptxas -O1: higher ptxas levels decode
+    # stereo SILK wrongly (decode_kernel.cu explains); the rest is -O3.
+    _run(common + ["-Xptxas", "-O1,-v", "-c", os.path.join(CSRC, "decode_kernel.cu"),
+                   "-o", os.path.join(obj, "decode_kernel.o")])
+    _run(common + ["-Xptxas", "-v", "-c", os.path.join(CSRC, "libcuopus.cu"), "-o", os.path.join(obj, "libcuopus.o")])
+    _run(common + ["-c", os.path.join(CSRC, "ogg_demux.cpp"), "-o", os.path.join(obj, "ogg_demux.o")])
     tmp = LIBCUOPUS + ".tmp"
-    _run([NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xptxas", "-v", "-Xcompiler", "-fPIC,-O2",
-          "-shared", "-I", CSRC, os.path.join(CSRC, "libcuopus.cu"), os.path.join(CSRC, "ogg_demux.cpp"),
-          "-o", tmp])
+    _run([NVCC, *ARCH, "-shared", "-o", tmp] +
+         [os.path.join(obj, o) for o in ("decode_kernel.o", "libcuopus.o", "ogg_demux.o")])
     os.replace(tmp, LIBCUOPUS)
     return LIBCUOPUS
 

@@ -23,11 +23,11 @@
 #include <string.h>
 
 #ifdef __CUDACC__
-#define DFN __device__ __forceinline__
+#define DFN static __device__ __forceinline__
 #define MFN __device__ __forceinline__
-#define DNI __device__ __noinline__
-#define TABC(type, decl) __constant__ type decl
-#define TABG(type, decl) __device__ const type decl
+#define DNI static __device__ __noinline__
+#define TABC(type, decl) static __constant__ type decl
+#define TABG(type, decl) static __device__ const type decl
 #else
 #define DFN static inline
 #define MFN inline

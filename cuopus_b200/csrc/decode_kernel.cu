@@ -1,0 +1,31 @@
+// Translation unit of the chain decoder kernel (k_decode_chains).
+//
+// It is compiled apart from the rest of libcuopus because its ptxas
+// optimisation level differs: at ptxas -O2 and -O3 this kernel decodes
+// stereo SILK and hybrid frames with wrong samples (the mid/side to left/right
+// stage diverges from libopus on the first stereo frame), while ptxas -O0 and
+// -O1, nvcc -G, and the same sources built for the host with g++ (also under
+// AddressSanitizer and UndefinedBehaviorSanitizer, and with every local
+// variable pattern-initialised) are bit-exact.  The stage in isolation is
+// bit-exact at every level, so the fault is in the optimised kernel as a
+// whole; build.py compiles this file with -Xptxas -O1 and the GPU parity
+// tests hold the kernel to libopus on stereo streams.
+#define CUO_DECODE_KERNEL_TU 1
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+
+namespace cuo {
+
+cudaError_t decode_kernel_occupancy(int block, int *blocks_per_sm)
+{
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_decode_chains, block, 0);
+}
+
+cudaError_t decode_kernel_launch(const DecodeArgs &a, int blocks, int block, cudaStream_t st)
+{
+    k_decode_chains<<<blocks, block, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+} // namespace cuo

@@ -6,6 +6,7 @@
 #include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
+#include <string.h>
 
 #include "dec/chain.cuh"
 
@@ -31,8 +32,11 @@ struct hc_job {
 static void *hc_worker(void *arg)
 {
     hc_job *j = (hc_job *)arg;
-    cuo::ChainSlot *slot = (cuo::ChainSlot *)calloc(1, sizeof(cuo::ChainSlot));
+    cuo::ChainSlot *slot = (cuo::ChainSlot *)malloc(sizeof(cuo::ChainSlot));
     if (!slot) return nullptr;
+    // poison the slot like fresh device memory: the decoder must not read
+    // anything it has not initialised
+    memset(slot, 0xA5, sizeof(cuo::ChainSlot));
     cuo::Lanes L{0, 1, 1u};
     for (;;) {
         pthread_mutex_lock(&j->mu);

@@ -44,6 +44,12 @@ struct DecodeArgs {
     int use_queue;
 };
 
+// Decoder kernel: defined in decode_kernel.cu, which is compiled on its own
+// (see the note there); the host side reaches it through these two calls.
+cudaError_t decode_kernel_occupancy(int block, int *blocks_per_sm);
+cudaError_t decode_kernel_launch(const DecodeArgs &a, int blocks, int block, cudaStream_t st);
+
+#ifdef CUO_DECODE_KERNEL_TU
 __global__ void __launch_bounds__(128) k_decode_chains(DecodeArgs a)
 {
     const int W = a.width;
@@ -78,7 +84,9 @@ __global__ void __launch_bounds__(128) k_decode_chains(DecodeArgs a)
         if (L.id == 0) a.res[c].cycles = (uint32_t)min(t1 - t0, 0xffffffffLL);
     }
 }
+#endif
 
+#ifndef CUO_DECODE_KERNEL_TU
 enum { RS_TAPS = 49, RS_PAD = 24, RS_OUT_PER_THREAD = 4, RS_THREADS = 256,
        RS_TILE_OUT = RS_THREADS * RS_OUT_PER_THREAD, RS_TILE_IN = 3 * RS_TILE_OUT + RS_TAPS - 1 };
 
@@ -115,5 +123,6 @@ __global__ void __launch_bounds__(RS_THREADS) k_resample48to16(const int16_t *__
             if (i0 + k < n_out) out[i0 + k] = acc[k];
     }
 }
+#endif
 
 } // namespace cuo

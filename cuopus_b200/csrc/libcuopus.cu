@@ -189,7 +189,7 @@ int ensure_occupancy(Err &err)
     CK(cudaGetDevice(&dev));
     if (G.occ_dev == dev) return RC_OK;
     CK(cudaDeviceGetAttribute(&G.sm_count, cudaDevAttrMultiProcessorCount, dev));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&G.occ_blocks, cuo::k_decode_chains, BLOCK, 0));
+    CK(cuo::decode_kernel_occupancy(BLOCK, &G.occ_blocks));
     if (G.occ_blocks < 1) G.occ_blocks = 1;
     G.occ_dev = dev;
     return RC_OK;
@@ -260,8 +260,7 @@ int decode_batch(const cuopus_batch *b, cudaStream_t st, float *kernel_ms, Err &
     a.width = width;
     a.use_queue = b->schedule == 1;
     CK(cudaEventRecord(G.ev0, st));
-    cuo::k_decode_chains<<<blocks, BLOCK, 0, st>>>(a);
-    CK(cudaGetLastError());
+    CK(cuo::decode_kernel_launch(a, blocks, BLOCK, st));
     CK(cudaEventRecord(G.ev1, st));
     if (kernel_ms) {
         CK(cudaEventSynchronize(G.ev1));
