@@ -83,3 +83,52 @@ int hc_decode_chains(const uint8_t *data, const uint64_t *off, const uint32_t *l
 unsigned long hc_slot_bytes(void) { return sizeof(cuo::ChainSlot); }
 
 }
+
+// The range-decoder gate schedules (147 and 163 words) run through the
+// decoder's own range decoder (dec/rangedec.cuh); the oracle runs the same
+// schedules through libopus (oref_ec_schedule, oref_ec_schedule2).
+extern "C" {
+
+void hc_ec_schedule(const uint8_t *buf, uint32_t len, uint32_t *out)
+{
+    static const uint8_t icdf_tab[8] = {120, 112, 96, 64, 32, 16, 8, 0};
+    cuo::RangeDec d;
+    int k = 0;
+    cuo::rd_init(&d, buf, len);
+    for (int i = 0; i < 64; i++) out[k++] = (uint32_t)cuo::rd_bit_logp(&d, 1);
+    for (int i = 0; i < 32; i++) out[k++] = (uint32_t)cuo::rd_icdf(&d, icdf_tab, 7);
+    for (int i = 0; i < 32; i++) out[k++] = cuo::rd_uint(&d, 2000);
+    for (int i = 0; i < 16; i++) out[k++] = cuo::rd_bits(&d, 11);
+    out[k++] = (uint32_t)cuo::rd_tell(&d);
+    out[k++] = d.rng;
+    out[k++] = (uint32_t)d.error;
+}
+
+void hc_ec_schedule2(const uint8_t *buf, uint32_t len, uint32_t *out)
+{
+    static const uint8_t icdf_tab[8] = {200, 150, 100, 60, 30, 12, 4, 0};
+    cuo::RangeDec d;
+    int k = 0;
+    cuo::rd_init(&d, buf, len);
+    for (int i = 0; i < 16; i++) {
+        unsigned fs = 2000 + 1500 * (unsigned)(i & 7);
+        int decay = 6000 + 1000 * (i & 7);
+        out[k++] = (uint32_t)cuo::rd_laplace(&d, fs, decay);
+        unsigned s = cuo::rd_decode_bin(&d, 9);
+        cuo::rd_update(&d, s, s + 1, 512);
+        out[k++] = s;
+        out[k++] = (uint32_t)cuo::rd_bit_logp(&d, 1 + (i & 3));
+        out[k++] = (uint32_t)cuo::rd_icdf(&d, icdf_tab, 8);
+        out[k++] = cuo::rd_uint(&d, 3 + (unsigned)i);
+        out[k++] = cuo::rd_uint(&d, 70000u + 977u * (unsigned)i);
+        out[k++] = cuo::rd_bits(&d, 1 + (unsigned)(i % 16));
+        out[k++] = cuo::rd_tell_frac(&d);
+        out[k++] = (uint32_t)cuo::rd_tell(&d);
+        out[k++] = d.rng;
+    }
+    out[k++] = cuo::rd_tell_frac(&d);
+    out[k++] = d.rng;
+    out[k++] = (uint32_t)d.error;
+}
+
+}

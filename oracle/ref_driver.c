@@ -194,3 +194,57 @@ int oref_encode(const int16_t *pcm, int64_t n, int channels, const oref_seg *seg
 
 /* libopus version string of the oracle build, for logs. */
 const char *oref_version(void) { return opus_get_version_string(); }
+
+/* ------------------------------------------------------------------ range decoder schedules */
+
+#include "entdec.h"
+#include "laplace.h"
+
+/* The reference's phase-1 range-decoder gate (schedule.inc:18-36) run through
+ * libopus celt/entdec.c: on one buffer, 64 ec_dec_bit_logp(1), 32
+ * ec_dec_icdf({120,112,96,64,32,16,8,0}, 7), 32 ec_dec_uint(2000), 16
+ * ec_dec_bits(11), then ec_tell, rng and error: 147 words. */
+void oref_ec_schedule(const uint8_t *buf, uint32_t len, uint32_t *out)
+{
+    static const unsigned char icdf_tab[8] = {120, 112, 96, 64, 32, 16, 8, 0};
+    ec_dec dec;
+    int i, k = 0;
+    ec_dec_init(&dec, (unsigned char *)buf, len);
+    for (i = 0; i < 64; i++) out[k++] = (uint32_t)ec_dec_bit_logp(&dec, 1);
+    for (i = 0; i < 32; i++) out[k++] = (uint32_t)ec_dec_icdf(&dec, icdf_tab, 7);
+    for (i = 0; i < 32; i++) out[k++] = (uint32_t)ec_dec_uint(&dec, 2000);
+    for (i = 0; i < 16; i++) out[k++] = (uint32_t)ec_dec_bits(&dec, 11);
+    out[k++] = (uint32_t)ec_tell(&dec);
+    out[k++] = dec.rng;
+    out[k++] = (uint32_t)dec.error;
+}
+
+/* A wider schedule over the same entry points plus those the gate leaves out
+ * (ec_decode_bin + ec_dec_update, ec_laplace_decode, ec_tell_frac, small and
+ * large ec_dec_uint): 16 rounds of 10 words, then tell_frac, rng, error. */
+void oref_ec_schedule2(const uint8_t *buf, uint32_t len, uint32_t *out)
+{
+    static const unsigned char icdf_tab[8] = {200, 150, 100, 60, 30, 12, 4, 0};
+    ec_dec dec;
+    int i, k = 0;
+    ec_dec_init(&dec, (unsigned char *)buf, len);
+    for (i = 0; i < 16; i++) {
+        unsigned fs = 2000 + 1500 * (unsigned)(i & 7);
+        int decay = 6000 + 1000 * (i & 7);
+        out[k++] = (uint32_t)ec_laplace_decode(&dec, fs, decay);
+        unsigned s = ec_decode_bin(&dec, 9);
+        ec_dec_update(&dec, s, s + 1, 512);
+        out[k++] = s;
+        out[k++] = (uint32_t)ec_dec_bit_logp(&dec, 1 + (i & 3));
+        out[k++] = (uint32_t)ec_dec_icdf(&dec, icdf_tab, 8);
+        out[k++] = ec_dec_uint(&dec, 3 + (unsigned)i);
+        out[k++] = ec_dec_uint(&dec, 70000u + 977u * (unsigned)i);
+        out[k++] = ec_dec_bits(&dec, 1 + (unsigned)(i % 16));
+        out[k++] = ec_tell_frac(&dec);
+        out[k++] = (uint32_t)ec_tell(&dec);
+        out[k++] = dec.rng;
+    }
+    out[k++] = ec_tell_frac(&dec);
+    out[k++] = dec.rng;
+    out[k++] = (uint32_t)dec.error;
+}

@@ -10,8 +10,8 @@
  *         acc = fma(taps[t], x, acc) with x = in[3i - 24 + t] / 32768 and
  *         samples outside [0, avail) read as 0 (nvcc contracts acc += a*b to an
  *         FMA; fmaf here is the same correctly rounded operation).
- * orp_resample_f64 applies the same taps in double, and orp_resample_ideal an
- * ideal (double) windowed sinc, for error reporting.
+ * orp_resample_f64 applies the double-precision taps in double (the FP64 oracle
+ * the fp32 error is reported against).
  */
 #include <math.h>
 #include <stdint.h>

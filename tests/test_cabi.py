@@ -1,0 +1,73 @@
+"""The C ABI library loads on a machine without a GPU and exports every entry
+point include/cuopus.h declares (no compute call is made here)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "cuopus.h")
+LIB = os.path.join(ROOT, "cuopus_b200", "lib", "libcuopus.so")
+
+REFERENCE_EIGHT = ["cuopus_probe", "cuopus_decode_f16k", "cuopus_decode_f16k_on", "cuopus_decode_f16k_multi",
+                   "cuopus_warmup", "cuopus_last_arena_overflow", "cuopus_workspace_bytes",
+                   "cuopus_release_workspaces"]
+
+
+def declared():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(cuopus_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_the_reference_surface():
+    names = declared()
+    for n in REFERENCE_EIGHT:
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    assert os.path.exists(LIB), "libcuopus.so must be built (python -m cuopus_b200.build)"
+    lib = ctypes.CDLL(LIB)
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", LIB], capture_output=True, text=True).stdout
+    exported = set(l.split()[-1] for l in out.splitlines() if l.strip())
+    assert set(declared()) <= exported
+
+
+def test_python_surface_matches_reference_module():
+    from cuopus_b200 import cuopus_native as cn
+    for name in ("probe", "decode_ogg_to_cuda_tensor", "decode_ogg_multi", "warmup", "workspace_bytes",
+                 "last_arena_overflow", "release_workspaces", "CuopusError"):
+        assert hasattr(cn, name), name
+
+
+def test_host_only_calls_without_gpu():
+    """Calls that never touch the device work on a CPU-only machine."""
+    from cuopus_b200 import cuopus_native as cn
+    assert cn.workspace_bytes() >= 0
+    assert cn.last_arena_overflow() in (False, True)
+    assert cn.lib().cuopus_slot_bytes() > 0
+    assert cn.lib().cuopus_default_width() in (1, 2, 4, 8, 16, 32)
+
+
+def test_no_cpu_fallback_on_the_decode_path():
+    """Without a GPU the decode entry points fail with a CUDA error code,
+    never by decoding on the host."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from cuopus_b200 import cuopus_native as cn
+    data = open(os.path.join(ROOT, "tests", "golden", "streams", "plain_a.opus"), "rb").read()
+    n16 = cn.probe(data)
+    lib = cn.lib()
+    buf = (ctypes.c_float * n16)()
+    out_len = ctypes.c_int64(0)
+    err = ctypes.create_string_buffer(256)
+    rc = lib.cuopus_decode_f16k_on(data, len(data), ctypes.cast(buf, ctypes.c_void_p), n16,
+                                   ctypes.byref(out_len), None, err, 256)
+    assert rc == 2, (rc, err.value)
+    assert out_len.value == 0

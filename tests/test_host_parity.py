@@ -1,0 +1,228 @@
+"""Host-side parity (CPU only): the product's host code and the decoder's
+host same-source build against the golden fixtures and the oracle.
+
+* the C++ demuxer and chain builder of libcuopus.so (cuopus_index,
+  cuopus_probe, cuopus_probe_pcm) against the reference indexer's tables,
+  including its error returns on damaged input;
+* the decoder sources compiled for the host (libcuopus_hostcheck.so, one lane
+  per chain) against libopus: the range-decoder gate schedules and whole
+  chains (per-packet sample counts, final ranges, every int16 sample).  This
+  is the reference's "host same-source gate" (harness_host.cpp): it separates
+  "the restatement is right" from "the CUDA execution is right".
+"""
+import ctypes
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import corpus, ogg_port, ref_decode
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+HOSTCHECK = os.path.join(ROOT, "cuopus_b200", "lib", "libcuopus_hostcheck.so")
+
+with open(os.path.join(GOLD, "index.json")) as _f:
+    INDEX = json.load(_f)
+with open(os.path.join(GOLD, "decode.json")) as _f:
+    DECODE = json.load(_f)
+
+
+def _stream(name):
+    with open(os.path.join(GOLD, "streams", name + ".opus"), "rb") as f:
+        return f.read()
+
+
+@pytest.fixture(scope="module")
+def cn():
+    from cuopus_b200 import cuopus_native
+    try:
+        cuopus_native.lib()
+    except OSError as e:
+        pytest.fail("libcuopus.so must be built (python -m cuopus_b200.build): %s" % e)
+    return cuopus_native
+
+
+@pytest.fixture(scope="module")
+def hc():
+    if not os.path.exists(HOSTCHECK):
+        pytest.fail("libcuopus_hostcheck.so must be built (python -m cuopus_b200.build)")
+    return ctypes.CDLL(HOSTCHECK)
+
+
+# ------------------------------------------------------------------ demuxer
+
+@pytest.mark.parametrize("name", sorted(INDEX))
+def test_cxx_demuxer_matches_reference_indexer(cn, name):
+    g = INDEX[name]
+    data = _stream(name)
+    for seg, pre, key in ((1.0, 250.0, "chains_1_250"), (0.5, 80.0, "chains_0.5_80")):
+        ix = cn.index(data, seg_s=seg, preroll_ms=pre)
+        assert ix.channels == g["channels"]
+        assert ix.play48 == g["pcm_samples_48k"]
+        assert [int(v) for v in ix.pkt_len] == g["packet_len"]
+        assert hashlib.sha256(ix.blob.tobytes()).hexdigest() == g["packets_sha256"]
+        chains = [[int(a), int(b), int(c), int(d)] for a, b, c, d in zip(ix.first, ix.npkts, ix.trim, ix.keep)]
+        assert chains == g[key]
+
+
+@pytest.mark.parametrize("name", sorted(INDEX))
+def test_probe_lengths(cn, name):
+    g = INDEX[name]
+    data = _stream(name)
+    play, ch = cn.probe_pcm(data)
+    assert (play, ch) == (g["pcm_samples_48k"], g["channels"])
+    if g["channels"] == 1:
+        assert cn.probe(data) == max(0, (g["pcm_samples_48k"] - 48) // 3)
+    else:
+        with pytest.raises(cn.CuopusError) as e:
+            cn.probe(data)
+        assert e.value.rc == 1
+
+
+def test_probe_errors(cn):
+    data = _stream("plain_a")
+    with pytest.raises(cn.CuopusError) as e:      # not Ogg at all
+        cn.probe(b"\x00" * 100)
+    assert e.value.rc == 1
+    with pytest.raises(cn.CuopusError) as e:      # OpusHead page only
+        cn.probe(data[:60])
+    assert e.value.rc == 1
+    bad = bytearray(data)                         # wrong magic in the header packet
+    i = bad.find(b"OpusHead")
+    bad[i:i + 8] = b"OpusHexd"
+    with pytest.raises(cn.CuopusError) as e:
+        cn.probe(bytes(bad))
+    assert e.value.rc == 1
+    lib = cn.lib()                                # NULL output pointer: caller error
+    err = ctypes.create_string_buffer(64)
+    assert lib.cuopus_probe(data, len(data), None, err, 64) == 3
+    assert err.value
+    n16 = ctypes.c_int64(0)                       # NULL errbuf is tolerated
+    assert lib.cuopus_probe(data, len(data), ctypes.byref(n16), None, 0) == 0
+    assert n16.value == (INDEX["plain_a"]["pcm_samples_48k"] - 48) // 3
+
+
+def test_granule_mismatch_is_rejected(cn):
+    """A page granule that disagrees with the TOC durations fails the
+    cross-check (reference cuopus_demux.h:216-262)."""
+    data = bytearray(_stream("mixed_mono_b"))
+    pages = []
+    p = data.find(b"OggS")
+    while p >= 0:
+        pages.append(p)
+        p = data.find(b"OggS", p + 4)
+    mid = pages[len(pages) // 2]
+    g = int.from_bytes(data[mid + 6:mid + 14], "little")
+    data[mid + 6:mid + 14] = (g + 480).to_bytes(8, "little")
+    with pytest.raises(cn.CuopusError) as e:
+        cn.probe_pcm(bytes(data))
+    assert e.value.rc == 1
+
+
+# ------------------------------------------------------------------ host same-source decoder
+
+def test_range_decoder_gate_schedules(hc):
+    with open(os.path.join(GOLD, "rangedec.json")) as f:
+        cases = json.load(f)
+    for case in cases:
+        b = bytes.fromhex(case["buf"])
+        arr = np.frombuffer(b + b"\0", np.uint8)
+        o1 = np.zeros(147, np.uint32)
+        o2 = np.zeros(163, np.uint32)
+        hc.hc_ec_schedule(ctypes.c_void_p(arr.ctypes.data), len(b), ctypes.c_void_p(o1.ctypes.data))
+        hc.hc_ec_schedule2(ctypes.c_void_p(arr.ctypes.data), len(b), ctypes.c_void_p(o2.ctypes.data))
+        assert [int(x) for x in o1] == case["gate"]
+        assert [int(x) for x in o2] == case["wide"]
+
+
+def host_decode(hc, packets, chains, ch, nthreads=4):
+    """Decode chains with the host build; returns per chain (pcm, nsamp, rng, stop, samples)."""
+    blob, off, lens = ref_decode.flatten(packets)
+    n = len(chains)
+    first = np.array([c[0] for c in chains], np.uint32)
+    npk = np.array([c[1] for c in chains], np.uint32)
+    chans = np.full(n, ch, np.int32)
+    cap = np.array([sum(ogg_port.toc_samples48(packets[int(first[i]) + k]) for k in range(int(npk[i])))
+                    for i in range(n)], np.uint64)
+    pcm_off = np.zeros(n, np.uint64)
+    pcm_off[1:] = np.cumsum(cap[:-1] * ch)
+    pcm = np.zeros(int(cap.sum()) * ch + 1, np.int16)
+    rec = np.zeros(n, np.uint64)
+    rec[1:] = np.cumsum(npk[:-1])
+    ns = np.zeros(int(npk.sum()) + 1, np.uint32)
+    rg = np.zeros_like(ns)
+    res = np.zeros(4 * n, np.uint32)
+    P = lambda a: ctypes.c_void_p(a.ctypes.data)
+    hc.hc_decode_chains(P(blob), P(off), P(lens), P(first), P(npk), P(chans), n, P(pcm), P(pcm_off), None, None,
+                        P(rec), P(ns), P(rg), P(res), nthreads)
+    res = res.reshape(-1, 4)
+    out = []
+    for i in range(n):
+        r0, k = int(rec[i]), int(npk[i])
+        p0 = int(pcm_off[i])
+        out.append((pcm[p0:p0 + int(res[i, 1]) * ch], ns[r0:r0 + k], rg[r0:r0 + k], int(np.int32(res[i, 0])),
+                    int(res[i, 1])))
+    return out
+
+
+@pytest.mark.parametrize("name", sorted(DECODE))
+def test_host_decoder_matches_golden_libopus(hc, name):
+    ix = ogg_port.demux(_stream(name))
+    chains = [tuple(c) for c in INDEX[name]["chains_1_250"]]
+    got = host_decode(hc, ix["packets"], chains, ix["channels"])
+    for i, g in enumerate(DECODE[name]):
+        pcm, ns, rg, stop, samples = got[i]
+        assert stop == g["status"] and samples == g["samples"], (name, i)
+        assert [int(v) for v in ns] == g["nsamp"], (name, i)
+        assert [int(v) for v in rg] == g["rng"], (name, i)
+        assert hashlib.sha256(pcm.astype("<i2").tobytes()).hexdigest() == g["pcm_sha256"], (name, i)
+
+
+@pytest.mark.parametrize("seed", [11, 12, 13, 14])
+def test_host_decoder_matches_libopus_mixed(hc, seed):
+    """Fresh seeded streams (SILK/hybrid/CELT, 2.5-60 ms, mono/stereo),
+    compared sample by sample with libopus."""
+    try:
+        corpus.ref_lib()
+    except OSError as e:
+        pytest.skip(str(e))
+    d = corpus.make_stream(dict(kind="mixed", seed=seed, seconds=3.0, channels=1 + seed % 2))
+    ix = ogg_port.demux(d)
+    chains = ogg_port.build_chains(ix, 1.0, 250.0)
+    ref = ref_decode.decode_chains(ix["packets"], chains, ix["channels"])
+    got = host_decode(hc, ix["packets"], chains, ix["channels"])
+    for i in range(len(chains)):
+        pcm, ns, rg, stop, _ = got[i]
+        assert stop == int(ref["status"][i]) == 0
+        assert np.array_equal(ns, ref["nsamp"][i]) and np.array_equal(rg, ref["rng"][i])
+        assert np.array_equal(pcm, ref["pcm"][i])
+
+
+def test_host_decoder_damaged_packets_match_libopus(hc):
+    """Truncated and bit-flipped packets: the decoder returns the same status,
+    sample counts and samples as libopus (errors stop the chain)."""
+    try:
+        corpus.ref_lib()
+    except OSError as e:
+        pytest.skip(str(e))
+    rng = np.random.default_rng(5)
+    ix = ogg_port.demux(_stream("mixed_stereo_a"))
+    pk = list(ix["packets"])
+    for i in range(0, len(pk), 7):
+        p = bytearray(pk[i])
+        if i % 3 == 0 and len(p) > 3:
+            p = p[: len(p) // 2]
+        elif len(p) > 2:
+            j = int(rng.integers(1, len(p)))
+            p[j] ^= 1 << int(rng.integers(0, 8))
+        pk[i] = bytes(p)
+    chains = [(0, len(pk))]
+    ref = ref_decode.decode_chains(pk, chains, ix["channels"])
+    got = host_decode(hc, pk, chains, ix["channels"])
+    pcm, ns, rg, stop, samples = got[0]
+    assert stop == int(ref["status"][0])
+    assert np.array_equal(ns, ref["nsamp"][0]) and np.array_equal(rg, ref["rng"][0])
+    assert np.array_equal(pcm, ref["pcm"][0])
