@@ -96,7 +96,7 @@ def build_cli(force=False):
     cuda = os.path.dirname(os.path.dirname(NVCC))
     _run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(cuda, "include"),
           src, "-o", CLI + ".tmp", "-L", LIB, "-lcuopus", "-Wl,-rpath,$ORIGIN/../lib",
-          "-L", os.path.join(cuda, "lib64"), "-lcudart", "-lpthread"])
+          "-L", os.path.join(cuda, "lib64"), "-lcudart_static", "-ldl", "-lrt", "-lpthread"])
     os.replace(CLI + ".tmp", CLI)
     return CLI
 

@@ -19,6 +19,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #include <algorithm>
 #include <cmath>
@@ -78,8 +79,11 @@ struct State {
     int occ_dev = -1, occ_blocks = 0, sm_count = 0;
     float last_kernel_ms = 0.f;
     int last_ovf = 0;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;     // decode kernel
+    cudaEvent_t evh0 = nullptr, evh1 = nullptr;   // packet / table upload
+    cudaEvent_t evr0 = nullptr, evr1 = nullptr;   // resampler
     int ev_dev = -1;
+    cuopus_stats last{};
 } G;
 
 std::mutex g_mu;
@@ -200,10 +204,17 @@ int ensure_events(Err &err)
     int dev = 0;
     CK(cudaGetDevice(&dev));
     if (G.ev_dev == dev && G.ev0) return RC_OK;
-    CK(cudaEventCreate(&G.ev0));
-    CK(cudaEventCreate(&G.ev1));
+    cudaEvent_t *evs[] = {&G.ev0, &G.ev1, &G.evh0, &G.evh1, &G.evr0, &G.evr1};
+    for (cudaEvent_t *e : evs) CK(cudaEventCreate(e));
     G.ev_dev = dev;
     return RC_OK;
+}
+
+double now_ms()
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
 }
 
 // ------------------------------------------------------------------ engine
@@ -353,6 +364,8 @@ int run_plan(const Plan &P, cudaStream_t st, Err &err)
     if ((rc = gpu_grow(G.res, 16ull * nch, err))) return rc;
     if ((rc = gpu_grow(G.pcm, 2ull * P.out_elems + 16, err))) return rc;
     // stage everything through one pinned buffer, then one async copy per table
+    if ((rc = ensure_events(err))) return rc;
+    CK(cudaEventRecord(G.evh0, st));
     uint8_t *h = (uint8_t *)G.hpin.p;
     size_t o = 0;
     auto stage = [&](Grow &dst, const void *src, size_t bytes) -> int {
@@ -372,6 +385,7 @@ int run_plan(const Plan &P, cudaStream_t st, Err &err)
     if ((rc = stage(G.trim, P.trim.data(), 8ull * nch))) return rc;
     if ((rc = stage(G.keep, P.keep.data(), 8ull * nch))) return rc;
     if ((rc = stage(G.out_off, P.out_off.data(), 8ull * nch))) return rc;
+    CK(cudaEventRecord(G.evh1, st));
     cuopus_batch b;
     memset(&b, 0, sizeof b);
     b.data = (const uint8_t *)G.data.p;
@@ -416,6 +430,10 @@ int validate(const Plan &P, cudaStream_t st, Err &err)
     return RC_OK;
 }
 
+// Timings of the call that just completed (its stream is synchronised).
+struct Plan;
+void record_stats(const Plan &P, bool resampled);
+
 int64_t out16_of(int64_t play48)
 {
     int64_t v = (int64_t)((play48 - (int64_t)SWR_TAIL_48K) / 3);
@@ -443,7 +461,10 @@ int f16k_impl(const uint8_t *const *oggs, const size_t *ns, int nfiles, float *c
     int rc = refuse_capture(st, err);
     if (rc) return rc;
     Plan P;
+    G.last = cuopus_stats{};
+    double t0 = now_ms();
     if ((rc = plan_files(oggs, ns, nfiles, true, P, err))) return rc;
+    G.last.demux_ms = now_ms() - t0;
     if (P.first.empty()) return err.set(RC_SOFT, "no chains");
     if (enforce_max_batch) {
         int max_batch = env_i("CUOPUS_MAX_BATCH", 2048);
@@ -463,18 +484,42 @@ int f16k_impl(const uint8_t *const *oggs, const size_t *ns, int nfiles, float *c
     for (int f = 0; f < nfiles; f++) total16 += n16[f];
     if (total16 == 0) return RC_OK;
     if ((rc = run_plan(P, st, err))) return rc;
+    CK(cudaEventRecord(G.evr0, st));
     for (int f = 0; f < nfiles; f++) {
         const int16_t *in = (const int16_t *)G.pcm.p + P.file_out0[f];
         if ((rc = resample(in, (int64_t)P.file_keep[f], n16[f], out_devs[f], st, err))) return rc;
     }
+    CK(cudaEventRecord(G.evr1, st));
     if ((rc = validate(P, st, err))) return rc;
+    record_stats(P, true);
     if (out_lens) for (int f = 0; f < nfiles; f++) out_lens[f] = n16[f];
     return RC_OK;
+}
+
+void record_stats(const Plan &P, bool resampled)
+{
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, G.evh0, G.evh1) == cudaSuccess) G.last.h2d_ms = ms;
+    if (cudaEventElapsedTime(&ms, G.ev0, G.ev1) == cudaSuccess) G.last.kernel_ms = ms;
+    if (resampled && cudaEventElapsedTime(&ms, G.evr0, G.evr1) == cudaSuccess) G.last.resample_ms = ms;
+    G.last.chains = (int64_t)P.first.size();
+    G.last.packets = (int64_t)P.len.size();
+    int64_t play = 0;
+    for (int64_t v : P.file_play48) play += v;
+    G.last.play48 = play;
+    cudaGetLastError();
 }
 
 } // namespace
 
 // ====================================================================== C ABI
+
+extern "C" int cuopus_last_stats(cuopus_stats *s)
+{
+    if (!s) return RC_ARG;
+    *s = G.last;
+    return RC_OK;
+}
 
 extern "C" int cuopus_last_arena_overflow(void) { return G.last_ovf; }
 
@@ -592,7 +637,10 @@ extern "C" int cuopus_decode_i16_multi(const uint8_t *const *oggs, const size_t 
     int rc = refuse_capture(st, err);
     if (rc) return rc;
     Plan P;
+    G.last = cuopus_stats{};
+    double t0 = now_ms();
     if ((rc = plan_files(oggs, ns, nfiles, false, P, err))) return rc;
+    G.last.demux_ms = now_ms() - t0;
     if (P.first.empty()) return err.set(RC_SOFT, "no chains");
     for (int f = 0; f < nfiles; f++) {
         uint64_t need = P.file_keep[f] * (uint64_t)P.file_chans[f];
@@ -609,6 +657,7 @@ extern "C" int cuopus_decode_i16_multi(const uint8_t *const *oggs, const size_t 
                                cudaMemcpyDeviceToDevice, st));
     }
     if ((rc = validate(P, st, err))) return rc;
+    record_stats(P, false);
     for (int f = 0; f < nfiles; f++) {
         if (out_lens) out_lens[f] = (int64_t)P.file_keep[f];
         if (out_channels) out_channels[f] = P.file_chans[f];

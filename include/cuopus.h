@@ -128,6 +128,22 @@ int cuopus_index(const uint8_t *ogg, size_t n, double seg_s, double preroll_ms, 
                  uint8_t *blob, uint64_t *pkt_off, uint32_t *pkt_len, uint32_t *first, uint32_t *npkts,
                  uint32_t *trim, uint32_t *keep, char *errbuf, size_t errcap);
 
+/* Extension: timings and sizes of the last successful decode call of the
+ * entry points above (the reference CLI's per-request report,
+ * decode_cli.cu:486-491, 656-664): host demux, upload, decode kernel and
+ * resampler times, chains, packets and playable samples at 48 kHz. */
+typedef struct cuopus_stats {
+    double demux_ms;
+    float h2d_ms;
+    float kernel_ms;
+    float resample_ms;
+    int64_t chains;
+    int64_t packets;
+    int64_t play48;
+} cuopus_stats;
+
+int cuopus_last_stats(cuopus_stats *s);
+
 /* Extension: bytes of device state per decoder slot, and the number of lanes
  * per chain the entry points use (CUOPUS_STRIDE, default 32). */
 long long cuopus_slot_bytes(void);
