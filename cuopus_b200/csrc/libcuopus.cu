@@ -77,6 +77,12 @@ struct State {
     long long dev_bytes = 0;
     int taps_dev = -1;
     int occ_dev = -1, occ_blocks = 0, sm_count = 0;
+    int occ_by_warps[5] = {0, 1, 1, 1, 1};       // resident blocks per SM by warps per block
+    // decode launch captured as a CUDA graph (queue reset + kernel) and its key
+    cudaGraphExec_t gexec = nullptr;
+    cudaStream_t cap_stream = nullptr;
+    int cap_dev = -1, g_dev = -1, g_blocks = 0, g_block = 0;
+    cuo::DecodeArgs g_args;
     float last_kernel_ms = 0.f;
     int last_ovf = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;     // decode kernel
@@ -187,16 +193,34 @@ int ensure_taps(cudaStream_t st, Err &err)
     return RC_OK;
 }
 
+// Resident blocks per SM of the decode kernel at the block sizes the engine
+// launches (32, 64, 96 or 128 threads), per device.
 int ensure_occupancy(Err &err)
 {
     int dev = 0;
     CK(cudaGetDevice(&dev));
     if (G.occ_dev == dev) return RC_OK;
     CK(cudaDeviceGetAttribute(&G.sm_count, cudaDevAttrMultiProcessorCount, dev));
-    CK(cuo::decode_kernel_occupancy(BLOCK, &G.occ_blocks));
-    if (G.occ_blocks < 1) G.occ_blocks = 1;
+    for (int w = 1; w <= 4; w++) {
+        int nb = 0;
+        CK(cuo::decode_kernel_occupancy(32 * w, &nb));
+        G.occ_by_warps[w] = nb < 1 ? 1 : nb;
+    }
+    G.occ_blocks = G.occ_by_warps[BLOCK / 32];
     G.occ_dev = dev;
     return RC_OK;
+}
+
+int block_threads(const cuopus_batch *b)
+{
+    int t = b->block > 0 ? b->block : BLOCK;
+    return t;
+}
+
+// Decoder groups resident on the whole GPU for a block size and width.
+long long resident_groups(int block, int width)
+{
+    return (long long)G.sm_count * G.occ_by_warps[block / 32] * (block / width);
 }
 
 int ensure_events(Err &err)
@@ -219,6 +243,55 @@ double now_ms()
 
 // ------------------------------------------------------------------ engine
 
+void drop_graph()
+{
+    if (G.gexec) cudaGraphExecDestroy(G.gexec);
+    G.gexec = nullptr;
+    G.g_dev = -1;
+}
+
+// The decode launch as a CUDA graph: the work-queue reset and the kernel,
+// captured once on a library-private stream and replayed on the caller's
+// stream.  The key is the full argument block and grid, so a launch with
+// other tables, sizes or workspaces captures again (the previous executable
+// graph is released first).
+int launch_graph(const cuo::DecodeArgs &a, int blocks, int block, cudaStream_t st, Err &err)
+{
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    bool hit = G.gexec && G.g_dev == dev && G.g_blocks == blocks && G.g_block == block &&
+               memcmp(&G.g_args, &a, sizeof a) == 0;
+    if (!hit) {
+        drop_graph();
+        if (!G.cap_stream || G.cap_dev != dev) {
+            CK(cudaStreamCreateWithFlags(&G.cap_stream, cudaStreamNonBlocking));
+            G.cap_dev = dev;
+        }
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(G.cap_stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e1 = a.use_queue ? cudaMemsetAsync(G.queue.p, 0, sizeof(unsigned), G.cap_stream) : cudaSuccess;
+        cudaError_t e2 = cuo::decode_kernel_launch(a, blocks, block, G.cap_stream);
+        cudaError_t e3 = cudaStreamEndCapture(G.cap_stream, &g);
+        if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaError_t e = e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3);
+            return err.set(RC_CUDA, "graph capture of the decode launch: %s", cudaGetErrorString(e));
+        }
+        cudaError_t e = cudaGraphInstantiate(&G.gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            G.gexec = nullptr;
+            return err.set(RC_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        }
+        G.g_dev = dev;
+        G.g_blocks = blocks;
+        G.g_block = block;
+        G.g_args = a;
+    }
+    CK(cudaGraphLaunch(G.gexec, st));
+    return RC_OK;
+}
+
 int decode_batch(const cuopus_batch *b, cudaStream_t st, float *kernel_ms, Err &err)
 {
     if (!b) return err.set(RC_ARG, "batch is NULL");
@@ -231,15 +304,24 @@ int decode_batch(const cuopus_batch *b, cudaStream_t st, float *kernel_ms, Err &
         return err.set(RC_ARG, "batch has a NULL table");
     if (b->out && !b->out_off) return err.set(RC_ARG, "out without out_off");
     if ((b->pkt_nsamp || b->pkt_rng) && !b->rec_off) return err.set(RC_ARG, "per-packet records without rec_off");
+    if (b->schedule < 0 || b->schedule > 2) return err.set(RC_ARG, "schedule %d is not 0, 1 or 2", b->schedule);
+    int block = block_threads(b);
+    if (block != 32 && block != 64 && block != 96 && block != 128)
+        return err.set(RC_ARG, "block %d is not 32, 64, 96 or 128 threads", block);
+    if (block % width) return err.set(RC_ARG, "width %d does not divide block %d", width, block);
     int rc = ensure_occupancy(err);
     if (rc) return rc;
     if ((rc = ensure_events(err))) return rc;
-    long long resident = (long long)G.sm_count * G.occ_blocks * (BLOCK / width);
-    long long groups = std::min<long long>(b->nchains, resident);
+    // plain: one group per chain, the hardware block scheduler assigns them;
+    // static / queue: a persistent grid of the resident groups
+    long long groups = b->schedule == 2 ? (long long)b->nchains
+                                        : std::min<long long>(b->nchains, resident_groups(block, width));
     if (b->max_groups > 0) groups = std::min<long long>(groups, b->max_groups);
-    int gpb = BLOCK / width;
-    int blocks = (int)((groups + gpb - 1) / gpb);
-    long long nslots = (long long)blocks * gpb;
+    int gpb = block / width;
+    long long blocks_ll = (groups + gpb - 1) / gpb;
+    if (blocks_ll > 0x7fffffffLL) return err.set(RC_ARG, "too many chains for one launch");
+    int blocks = (int)blocks_ll;
+    long long nslots = blocks_ll * gpb;
     if ((rc = gpu_grow(G.slots, (size_t)nslots * sizeof(cuo::ChainSlot), err))) return rc;
     if ((rc = gpu_grow(G.queue, sizeof(unsigned), err))) return rc;
     const uint32_t *order_dev = nullptr;
@@ -248,8 +330,8 @@ int decode_batch(const cuopus_batch *b, cudaStream_t st, float *kernel_ms, Err &
         CK(cudaMemcpyAsync(G.order.p, b->order, 4ull * b->nchains, cudaMemcpyHostToDevice, st));
         order_dev = (const uint32_t *)G.order.p;
     }
-    CK(cudaMemsetAsync(G.queue.p, 0, sizeof(unsigned), st));
     cuo::DecodeArgs a;
+    memset(&a, 0, sizeof a);
     a.data = b->data;
     a.off = b->off;
     a.len = b->len;
@@ -271,7 +353,12 @@ int decode_batch(const cuopus_batch *b, cudaStream_t st, float *kernel_ms, Err &
     a.width = width;
     a.use_queue = b->schedule == 1;
     CK(cudaEventRecord(G.ev0, st));
-    CK(cuo::decode_kernel_launch(a, blocks, BLOCK, st));
+    if (b->graph) {
+        if ((rc = launch_graph(a, blocks, block, st, err))) return rc;
+    } else {
+        if (a.use_queue) CK(cudaMemsetAsync(G.queue.p, 0, sizeof(unsigned), st));
+        CK(cuo::decode_kernel_launch(a, blocks, block, st));
+    }
     CK(cudaEventRecord(G.ev1, st));
     if (kernel_ms) {
         CK(cudaEventSynchronize(G.ev1));
@@ -528,6 +615,7 @@ extern "C" long long cuopus_workspace_bytes(void) { return G.dev_bytes; }
 extern "C" void cuopus_release_workspaces(void)
 {
     std::lock_guard<std::mutex> lk(g_mu);
+    drop_graph();
     Grow *all[] = {&G.data, &G.off, &G.len, &G.first, &G.npkts, &G.chans, &G.trim, &G.keep,
                    &G.out_off, &G.order, &G.res, &G.slots, &G.queue, &G.pcm};
     for (Grow *g : all) {
@@ -678,6 +766,54 @@ extern "C" int cuopus_decode_batch(const cuopus_batch *b, void *cuda_stream, flo
     return RC_OK;
 }
 
+// Autotuner: every (width, block) candidate decodes the batch as given
+// (schedule, order, graph) `reps` times; the candidate with the lowest
+// median kernel time wins.  Candidates whose launch is rejected are skipped.
+extern "C" int cuopus_autotune(const cuopus_batch *b, const int32_t *widths, int nwidths, const int32_t *blocks,
+                               int nblocks, int reps, void *cuda_stream, int32_t *best_width, int32_t *best_block,
+                               float *times_ms, char *errbuf, size_t errcap)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    Err err(errbuf, errcap);
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    if (!b || !widths || !blocks || nwidths <= 0 || nblocks <= 0 || !best_width || !best_block)
+        return err.set(RC_ARG, "autotune: bad arguments");
+    int rc = refuse_capture(st, err);
+    if (rc) return rc;
+    if (reps < 1) reps = 1;
+    float best = -1.f;
+    for (int i = 0; i < nwidths; i++)
+        for (int j = 0; j < nblocks; j++) {
+            cuopus_batch c = *b;
+            c.width = widths[i];
+            c.block = blocks[j];
+            std::vector<float> t;
+            bool ok = true;
+            for (int r = 0; r < reps && ok; r++) {
+                float ms = 0.f;
+                Err e2(nullptr, 0);
+                int rc2 = decode_batch(&c, st, &ms, e2);
+                if (rc2 == RC_CUDA) return err.set(rc2, "autotune: %s", e2.buf);
+                ok = rc2 == RC_OK;
+                t.push_back(ms);
+            }
+            float med = -1.f;
+            if (ok) {
+                std::sort(t.begin(), t.end());
+                med = t[t.size() / 2];
+                if (best < 0.f || med < best) {
+                    best = med;
+                    *best_width = c.width;
+                    *best_block = c.block;
+                }
+            }
+            if (times_ms) times_ms[i * nblocks + j] = med;
+        }
+    CK(cudaStreamSynchronize(st));
+    if (best < 0.f) return err.set(RC_ARG, "autotune: no candidate could be launched");
+    return RC_OK;
+}
+
 extern "C" int cuopus_resample48to16(const int16_t *in_dev, int64_t avail, int64_t n_out, float *out_dev,
                                      void *cuda_stream, char *errbuf, size_t errcap)
 {
@@ -700,7 +836,7 @@ extern "C" int cuopus_warmup(char *errbuf, size_t errcap)
     if (rc) return rc;
     if ((rc = ensure_events(err))) return rc;
     int width = default_width();
-    long long nslots = (long long)G.sm_count * G.occ_blocks * (BLOCK / width);
+    long long nslots = resident_groups(BLOCK, width);
     if ((rc = gpu_grow(G.slots, (size_t)nslots * sizeof(cuo::ChainSlot), err))) return rc;
     if ((rc = ensure_taps(nullptr, err))) return rc;
     CK(cudaDeviceSynchronize());

@@ -50,7 +50,7 @@ class Batch(ctypes.Structure):
                 ("out", ctypes.c_void_p), ("rec_off", ctypes.c_void_p), ("pkt_nsamp", ctypes.c_void_p),
                 ("pkt_rng", ctypes.c_void_p), ("res", ctypes.c_void_p), ("nchains", ctypes.c_int32),
                 ("width", ctypes.c_int32), ("schedule", ctypes.c_int32), ("max_groups", ctypes.c_int32),
-                ("order", ctypes.c_void_p)]
+                ("order", ctypes.c_void_p), ("block", ctypes.c_int32), ("graph", ctypes.c_int32)]
 
 
 _lib = None
@@ -84,6 +84,12 @@ def _load():
     lib.cuopus_decode_batch.restype = ctypes.c_int
     lib.cuopus_decode_batch.argtypes = [ctypes.POINTER(Batch), c_p, ctypes.POINTER(ctypes.c_float),
                                         ctypes.c_char_p, ctypes.c_size_t]
+    lib.cuopus_autotune.restype = ctypes.c_int
+    lib.cuopus_autotune.argtypes = [ctypes.POINTER(Batch), c_p, ctypes.c_int, c_p, ctypes.c_int, ctypes.c_int, c_p,
+                                    ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), c_p,
+                                    ctypes.c_char_p, ctypes.c_size_t]
+    lib.cuopus_last_stats.restype = ctypes.c_int
+    lib.cuopus_last_stats.argtypes = [c_p]
     lib.cuopus_resample48to16.restype = ctypes.c_int
     lib.cuopus_resample48to16.argtypes = [c_p, ctypes.c_int64, ctypes.c_int64, c_p, c_p, ctypes.c_char_p,
                                           ctypes.c_size_t]
@@ -261,6 +267,38 @@ def decode_batch(batch: Batch, stream=None):
     _check(lib.cuopus_decode_batch(ctypes.byref(batch), ctypes.c_void_p(stream or 0), ctypes.byref(ms), err,
                                    _ERRCAP), err)
     return ms.value
+
+
+def autotune(batch: Batch, widths=(4, 8, 16, 32), blocks=(32, 64, 128), reps=1, stream=None):
+    """Extension: time the batch at every (width, block) pair; returns
+    (best_width, best_block, {(width, block): median ms or None})."""
+    import numpy as np
+    lib = _load()
+    w = np.ascontiguousarray(np.array(widths, np.int32))
+    b = np.ascontiguousarray(np.array(blocks, np.int32))
+    t = np.zeros(len(w) * len(b), np.float32)
+    bw, bb = ctypes.c_int32(0), ctypes.c_int32(0)
+    err = ctypes.create_string_buffer(_ERRCAP)
+    _check(lib.cuopus_autotune(ctypes.byref(batch), w.ctypes.data, len(w), b.ctypes.data, len(b), int(reps),
+                               ctypes.c_void_p(stream or 0), ctypes.byref(bw), ctypes.byref(bb), t.ctypes.data,
+                               err, _ERRCAP), err)
+    table = {(int(w[i]), int(b[j])): (float(t[i * len(b) + j]) if t[i * len(b) + j] >= 0 else None)
+             for i in range(len(w)) for j in range(len(b))}
+    return bw.value, bb.value, table
+
+
+class Stats(ctypes.Structure):
+    """cuopus_stats of include/cuopus.h."""
+    _fields_ = [("demux_ms", ctypes.c_double), ("h2d_ms", ctypes.c_float), ("kernel_ms", ctypes.c_float),
+                ("resample_ms", ctypes.c_float), ("chains", ctypes.c_int64), ("packets", ctypes.c_int64),
+                ("play48", ctypes.c_int64)]
+
+
+def last_stats():
+    """Extension: timings of the last successful decode call (dict)."""
+    s = Stats()
+    _load().cuopus_last_stats(ctypes.byref(s))
+    return {k: getattr(s, k) for k, _ in Stats._fields_}
 
 
 def warmup():

@@ -77,9 +77,14 @@ int cuopus_decode_i16_multi(const uint8_t *const *oggs, const size_t *ns, int nf
 
 /* Extension: device-resident batch decode, the engine under every entry
  * above.  All pointers are device pointers unless noted.  Chains are decoded
- * by groups of `width` lanes; `schedule` 0 = static (chain c on group
- * c mod groups), 1 = device work queue in `order` (host pointer or NULL =
- * identity).  `max_groups` bounds the resident groups (0 = fill the GPU).
+ * by groups of `width` lanes (1..32, a power of two: the reference's
+ * "stride"); blocks have `block` threads (32, 64, 96 or 128; 0 = 128).
+ * `schedule` 0 = static persistent grid (chain c on group c mod groups),
+ * 1 = persistent grid pulling from a device work queue in `order` (host
+ * pointer or NULL = identity), 2 = plain one-launch form (one group per
+ * chain, the reference kernel's layout).  `max_groups` bounds the groups
+ * (0 = fill the GPU).  `graph` != 0 replays the launch (queue reset +
+ * kernel) as a CUDA graph, captured on first use for these arguments.
  * pkt_nsamp / pkt_rng (device, may be NULL) receive per-packet sample counts
  * and final ranges at rec_off[c] + k.  res: 4 x uint32 per chain
  * {stop, samples, final_range, cycles}.  kernel_ms (host, may be NULL)
@@ -104,9 +109,20 @@ typedef struct cuopus_batch {
     int32_t schedule;
     int32_t max_groups;
     const uint32_t *order;
+    int32_t block;
+    int32_t graph;
 } cuopus_batch;
 
 int cuopus_decode_batch(const cuopus_batch *b, void *cuda_stream, float *kernel_ms, char *errbuf, size_t errcap);
+
+/* Extension: autotuner of the decode launch.  Decodes the batch `reps` times
+ * for every width in widths[0..nwidths) and block size in blocks[0..nblocks)
+ * (the schedule, order and graph flag of *b are kept) and returns the pair
+ * with the lowest median kernel time.  times_ms (host, may be NULL) receives
+ * nwidths x nblocks medians, -1 where the launch was rejected. */
+int cuopus_autotune(const cuopus_batch *b, const int32_t *widths, int nwidths, const int32_t *blocks, int nblocks,
+                    int reps, void *cuda_stream, int32_t *best_width, int32_t *best_block, float *times_ms,
+                    char *errbuf, size_t errcap);
 
 /* Extension: fp32 48->16 kHz resample of a device int16 mono stream (the
  * kernel behind the f16k entries): out[i], i < n_out, from in[0..avail). */
