@@ -50,7 +50,11 @@ cudaError_t decode_kernel_occupancy(int block, int *blocks_per_sm);
 cudaError_t decode_kernel_launch(const DecodeArgs &a, int blocks, int block, cudaStream_t st);
 
 #ifdef CUO_DECODE_KERNEL_TU
-__global__ void __launch_bounds__(128) k_decode_chains(DecodeArgs a)
+// Resident 128-thread blocks per SM the register allocation is sized for.
+#ifndef CUO_MIN_BLOCKS
+#define CUO_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(128, CUO_MIN_BLOCKS) k_decode_chains(DecodeArgs a)
 {
     const int W = a.width;
     const int lane = threadIdx.x & 31;

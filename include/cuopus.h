@@ -124,6 +124,33 @@ int cuopus_autotune(const cuopus_batch *b, const int32_t *widths, int nwidths, c
                     int reps, void *cuda_stream, int32_t *best_width, int32_t *best_block, float *times_ms,
                     char *errbuf, size_t errcap);
 
+/* ---- Extension: learned cost model of the queue schedule (no counterpart in
+ * the reference).  An FP32 MLP 16 -> 64 -> 64 -> 1 (ReLU) predicts a chain's
+ * log decode cycles from 16 features of its packets' TOC bytes; chains are
+ * queued longest first by the prediction.  It orders work only: decoded
+ * samples do not depend on it.  All buffers are device pointers. */
+#define CUOPUS_MLP_FEATURES 16
+#define CUOPUS_MLP_HIDDEN 64
+#define CUOPUS_MLP_NPARAM (16 * 64 + 64 + 64 * 64 + 64 + 64 + 1)
+
+/* feat_dev[c * 16 + k]: log1p packets, log1p bytes, log1p frames, log1p
+ * seconds, channels - 1, SILK / hybrid / CELT frame fractions, 2.5 / 5 / 10 /
+ * 20 / >= 40 ms frame fractions, mean bandwidth / 4, stereo-flag packet
+ * fraction, log1p bytes per second; from the tables of *b. */
+int cuopus_chain_features(const cuopus_batch *b, float *feat_dev, void *cuda_stream, char *errbuf, size_t errcap);
+/* He-uniform weights from `seed`, zero biases. */
+int cuopus_mlp_init(float *params_dev, uint64_t seed, void *cuda_stream, char *errbuf, size_t errcap);
+/* y_dev[s] = network(x_dev[s * 16 ..]). */
+int cuopus_mlp_predict(const float *params_dev, const float *x_dev, int n, float *y_dev, void *cuda_stream,
+                       char *errbuf, size_t errcap);
+/* Gradient of mean_s (y_s - t_s)^2 in the parameter layout, and the loss. */
+int cuopus_mlp_grad(const float *params_dev, const float *x_dev, const float *t_dev, int n, float *grad_dev,
+                    float *loss_dev, void *cuda_stream, char *errbuf, size_t errcap);
+/* Full-batch Adam (steps rounded up to a multiple of 50, replayed as a CUDA
+ * graph); losses (host, may be NULL) receives the loss before each step. */
+int cuopus_mlp_train(float *params_dev, const float *x_dev, const float *t_dev, int n, int steps, float lr,
+                     float *losses, void *cuda_stream, char *errbuf, size_t errcap);
+
 /* Extension: fp32 48->16 kHz resample of a device int16 mono stream (the
  * kernel behind the f16k entries): out[i], i < n_out, from in[0..avail). */
 int cuopus_resample48to16(const int16_t *in_dev, int64_t avail, int64_t n_out, float *out_dev, void *cuda_stream,

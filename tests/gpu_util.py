@@ -3,6 +3,69 @@ engine (cuopus_decode_batch) through the C ABI."""
 import numpy as np
 
 
+def device_batch(packets_list, chains_list, channels_list):
+    """Device-resident tables of several streams' chains (no per-packet
+    records).  Returns (Batch, tensors to keep alive, meta dict)."""
+    import torch
+    from cuopus_b200 import cuopus_native as cn
+    from oracle.ogg_port import toc_samples48
+    blob, off, lens, first, npk, chans, trim, keep, cap = [], [], [], [], [], [], [], [], []
+    base_pkt = base_byte = 0
+    for pk, chs, ch in zip(packets_list, chains_list, channels_list):
+        for p in pk:
+            off.append(base_byte)
+            lens.append(len(p))
+            blob.append(p)
+            base_byte += len(p)
+        for c in chs:
+            first.append(c[0] + base_pkt)
+            npk.append(c[1])
+            chans.append(ch)
+            cp = sum(toc_samples48(pk[c[0] + k]) for k in range(c[1]))
+            t = c[2] if len(c) > 2 else 0
+            trim.append(t)
+            keep.append(min(c[3] if len(c) > 3 else cp, max(cp - t, 0)))
+            cap.append(cp)
+        base_pkt += len(pk)
+    n = len(first)
+    out_off = np.zeros(n, np.uint64)
+    if n > 1:
+        out_off[1:] = np.cumsum(np.array(keep[:-1], np.uint64) * np.array(chans[:-1], np.uint64))
+    total = int(sum(k * c for k, c in zip(keep, chans)))
+    t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(np.array(a, dtype=dt))).cuda()
+    T = dict(blob=t(np.frombuffer(b"".join(blob) + b"\0" * 16, np.uint8), np.uint8), off=t(off, np.uint64),
+             len=t(lens, np.uint32), first=t(first, np.uint32), npk=t(npk, np.uint32), ch=t(chans, np.uint8),
+             trim=t(trim, np.uint64), keep=t(keep, np.uint64), ooff=t(out_off, np.uint64),
+             out=torch.zeros(max(total, 1), dtype=torch.int16, device="cuda"),
+             res=torch.zeros(4 * max(n, 1), dtype=torch.int32, device="cuda"))
+    b = cn.Batch()
+    b.data, b.off, b.len = T["blob"].data_ptr(), T["off"].data_ptr(), T["len"].data_ptr()
+    b.first, b.npkts, b.channels = T["first"].data_ptr(), T["npk"].data_ptr(), T["ch"].data_ptr()
+    b.trim, b.keep, b.out_off = T["trim"].data_ptr(), T["keep"].data_ptr(), T["ooff"].data_ptr()
+    b.out, b.res = T["out"].data_ptr(), T["res"].data_ptr()
+    b.nchains = n
+    meta = dict(n=n, out_off=out_off, keep=np.array(keep), chans=np.array(chans), cap=np.array(cap),
+                npkts=np.array(npk), T=T)
+    return b, T, meta
+
+
+def run_device_batch(b, meta, width=32, schedule=1, order=None, block=0, graph=0):
+    """Run the engine on a device batch; returns res as uint32 [n, 4]."""
+    import torch
+    from cuopus_b200 import cuopus_native as cn
+    b.width, b.schedule, b.block, b.graph = width, schedule, block, graph
+    keep = None
+    if order is not None:
+        keep = np.ascontiguousarray(np.asarray(order, np.uint32))
+        b.order = keep.ctypes.data
+    else:
+        b.order = None
+    meta["T"]["res"].zero_()
+    cn.decode_batch(b, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    return meta["T"]["res"].cpu().numpy().view(np.uint32).reshape(-1, 4)[:meta["n"]]
+
+
 def run_batch(packets_list, chains_list, channels_list, width=32, schedule=0, order=None, max_groups=0,
               records=True):
     """Decode chains of several streams in one launch.

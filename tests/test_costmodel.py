@@ -1,0 +1,151 @@
+"""The scheduler's learned cost model: oracle pins (CPU), then the GPU
+features, forward pass and gradients against the oracle, training, and the
+makespan the trained model gains over the packet-count order."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mlp_port, ogg_port
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+
+
+def _rand_problem(seed, n=64):
+    rng = np.random.default_rng(seed)
+    p = rng.standard_normal(mlp_port.NPARAM) * 0.3
+    X = rng.standard_normal((n, 16))
+    T = rng.standard_normal(n)
+    return p, X, T
+
+
+def test_oracle_gradient_matches_finite_differences():
+    p, X, T = _rand_problem(1)
+    _, g = mlp_port.loss_and_grad(p, X, T)
+    rng = np.random.default_rng(2)
+    idx = np.concatenate([rng.choice(mlp_port.NPARAM, 60, replace=False), [mlp_port.OFF_B3]])
+    eps = 1e-6
+    for i in idx:
+        a, b = p.copy(), p.copy()
+        a[i] += eps
+        b[i] -= eps
+        fd = (mlp_port.loss_and_grad(a, X, T)[0] - mlp_port.loss_and_grad(b, X, T)[0]) / (2 * eps)
+        assert abs(fd - g[i]) <= 1e-6 + 1e-5 * abs(g[i]), i
+
+
+def test_oracle_features_are_consistent():
+    with open(os.path.join(GOLD, "index.json")) as f:
+        index = json.load(f)
+    for name in ("mixed_stereo_b", "plain_a", "code3_120ms"):
+        d = open(os.path.join(GOLD, "streams", name + ".opus"), "rb").read()
+        ix = ogg_port.demux(d)
+        chains = ogg_port.build_chains(ix, 1.0, 250.0)
+        f = mlp_port.features(ix["packets"], chains, ix["channels"])
+        assert f.shape == (len(chains), 16)
+        assert np.allclose(f[:, 5] + f[:, 6] + f[:, 7], 1.0, atol=1e-6)
+        assert np.allclose(f[:, 8:13].sum(1), 1.0, atol=1e-6)
+        assert np.allclose(f[:, 0], np.log1p([c[1] for c in chains]))
+        assert np.all(f[:, 4] == index[name]["channels"] - 1)
+
+
+def test_longest_first_makespan_on_skewed_costs():
+    """List scheduling longest-first is never worse than the lower bound by
+    more than the LPT factor 4/3, and beats index order on Pareto costs."""
+    rng = np.random.default_rng(3)
+    costs = 0.25 / (1.0 - rng.uniform(0, 1, 5000)) ** (1 / 1.5)
+    slots = 256
+    lpt = mlp_port.makespan(costs, np.argsort(-costs), slots)
+    idx = mlp_port.makespan(costs, np.arange(costs.size), slots)
+    lower = max(costs.max(), costs.sum() / slots)
+    assert lpt <= idx
+    assert lpt <= 4.0 / 3.0 * lower + 1e-9
+
+
+# ------------------------------------------------------------------ GPU
+
+@pytest.mark.gpu
+def test_gpu_features_match_oracle(cuda):
+    from cuopus_b200 import costmodel
+    from gpu_util import device_batch
+    names = ["mixed_stereo_a", "mixed_mono_b", "long_hybrid", "code3_120ms", "one_packet"]
+    pk, chs, nch = [], [], []
+    for name in names:
+        ix = ogg_port.demux(open(os.path.join(GOLD, "streams", name + ".opus"), "rb").read())
+        pk.append(ix["packets"])
+        chs.append(ogg_port.build_chains(ix, 1.0, 250.0))
+        nch.append(ix["channels"])
+    b, keep_alive, _ = device_batch(pk, chs, nch)
+    got = costmodel.chain_features(b).cpu().numpy()
+    want = np.concatenate([mlp_port.features(p, c, n) for p, c, n in zip(pk, chs, nch)])
+    assert got.shape == want.shape
+    assert np.allclose(got, want, rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.gpu
+def test_gpu_forward_and_gradient_match_oracle(cuda):
+    import torch
+    from cuopus_b200 import costmodel
+    p, X, T = _rand_problem(4, n=1000)
+    m = costmodel.CostModel()
+    m.params.copy_(torch.from_numpy(p.astype(np.float32)))
+    p32 = m.params.cpu().numpy().astype(np.float64)
+    Xd = torch.from_numpy(X.astype(np.float32)).cuda()
+    Td = torch.from_numpy(T.astype(np.float32)).cuda()
+    X32 = Xd.cpu().numpy().astype(np.float64)
+    T32 = Td.cpu().numpy().astype(np.float64)
+    y = m.predict_raw(Xd).cpu().numpy()
+    assert np.allclose(y, mlp_port.forward(p32, X32), rtol=1e-4, atol=1e-4)
+    loss, g = m.grad(Xd, Td)
+    want_loss, want_g = mlp_port.loss_and_grad(p32, X32, T32)
+    assert abs(loss - want_loss) <= 1e-4 * max(1.0, want_loss)
+    g = g.cpu().numpy()
+    scale = np.abs(want_g).max()
+    assert np.max(np.abs(g - want_g)) <= 1e-4 * scale
+    # deterministic reduction: the same call gives the same bits
+    _, g2 = m.grad(Xd, Td)
+    assert np.array_equal(g, g2.cpu().numpy())
+
+
+@pytest.mark.gpu
+def test_gpu_training_learns_decode_cost_and_beats_packet_order(cuda):
+    """Record per-chain decode cycles on a mixed batch, train on half, and
+    compare longest-first makespans on the other half: the learned order must
+    be at least as good as the packet-count order, and the fit must explain
+    most of the variance of log cycles."""
+    from cuopus_b200 import costmodel
+    from gpu_util import device_batch, run_device_batch
+    from oracle import corpus
+    rng = np.random.default_rng(11)
+    streams, chs = [], []
+    for s in range(160):
+        secs = float(min(0.25 / (1.0 - rng.uniform()) ** (1 / 1.5), 12.0))
+        ch = int(rng.integers(1, 3))
+        d = corpus.make_stream(dict(kind="mixed", seed=31000 + s, seconds=round(secs, 3), channels=ch))
+        ix = ogg_port.demux(d)
+        streams.append(ix)
+        chs.append([(0, len(ix["packets"]), 0, 1 << 40)])
+    b, keep_alive, meta = device_batch([ix["packets"] for ix in streams], chs, [ix["channels"] for ix in streams])
+    res = run_device_batch(b, meta, width=32, schedule=1)
+    cycles = res[:, 3].astype(np.float64)
+    assert np.all(res[:, 0] == 0) and np.all(cycles > 0)
+    X = costmodel.chain_features(b)
+    n = X.shape[0]
+    tr, te = np.arange(0, n, 2), np.arange(1, n, 2)
+    m = costmodel.CostModel(seed=5)
+    import torch
+    losses = m.fit(X[torch.from_numpy(tr).cuda()], cycles[tr], steps=1500, lr=3e-3)
+    assert losses[-1] < 0.25 * losses[0]
+    pred = m.predict(X[torch.from_numpy(te).cuda()])
+    y, yh = np.log(cycles[te]), np.log(pred)
+    r2 = 1.0 - np.sum((y - yh) ** 2) / np.sum((y - y.mean()) ** 2)
+    assert r2 > 0.7, r2
+    npk = np.array([len(streams[i]["packets"]) for i in te])
+    chans = np.array([streams[i]["channels"] for i in te])
+    slots = 8
+    ms_mlp = mlp_port.makespan(cycles[te], np.argsort(-pred, kind="stable"), slots)
+    ms_pkt = mlp_port.makespan(cycles[te], costmodel.packet_order(npk, chans), slots)
+    ms_opt_lb = max(cycles[te].max(), cycles[te].sum() / slots)
+    print("makespan mlp %.4g packet %.4g lower bound %.4g" % (ms_mlp, ms_pkt, ms_opt_lb))
+    assert ms_mlp <= ms_pkt * 1.001
