@@ -1,25 +1,33 @@
 #!/usr/bin/env python
 """Benchmark of the batched Opus decoder: audio-seconds decoded per second.
 
-Workload (default): the mixed-mode uneven batch - 4096 seeded synthetic Ogg Opus
-streams with log-uniform lengths 1-30 s, forced SILK / hybrid / CELT segments
-of 0.5-3 s, frames 2.5-60 ms, 6-128 kbps, mono or stereo; one chain per stream
-(4096 chains), decoded bit-exactly to int16 48 kHz PCM.  The reference's
-corpora are private; the streams are generated by the vendored libopus encoder
-(oracle/corpus.py) before anything is timed.
+Default workload (mixed4096): the mixed-mode uneven batch - 4096 seeded
+synthetic Ogg Opus streams with log-uniform lengths 1-30 s, forced SILK /
+hybrid / CELT segments of 0.5-3 s, frames 2.5-60 ms, 6-128 kbps, mono or
+stereo; one chain per stream, decoded bit-exactly to int16 48 kHz PCM.  The
+reference's corpora are private; the streams come from the vendored libopus
+encoder (oracle/corpus.py), generated before anything is timed.
 
 A step is one decode of the whole batch.
-  value   device-resident: packets and chain tables already in HBM, one call of
-          the engine (cuopus_decode_batch), CUDA-event timed on its stream.
-  e2e     through the public C ABI (cuopus_decode_i16_multi) from host Ogg
-          bytes: demux, host->device copy, decode, and a device->host read of
-          all decoded PCM into pinned memory, every step.
-  cpu_baseline  libopus 1.5.2 fixed point (the reference's CPU decoder, built
-          from its vendored sources) on all host cores, bounded sample.
---impl reference runs only that CPU decoder (the reference arm).
+  value      scheduled form: persistent grid pulling chains from a device work
+             queue, longest first by the learned cost model, replayed as a CUDA
+             graph, width x block picked by the autotuner; packets and chain
+             tables already in HBM; CUDA-event time on the launching stream
+  plain      the plain one-launch form on the same batch: one warp per chain,
+             one launch, chains in index order (the reference kernel's layout)
+  e2e        through the public C ABI (cuopus_decode_i16_multi) from host Ogg
+             bytes: demux, host->device copy, decode, and a device->host read of
+             all decoded PCM into pinned memory, every step
+  cpu_baseline  libopus 1.5.2 fixed point (the reference's own decoder,
+             compiled from its vendored sources) on all host cores, bounded
+             sample of the same workload
+Other workloads: pareto16384 (learned scheduling), long7200 (2 h mono file
+cut in 1 s chains, f16k), plain64, serve (Poisson arrivals through the
+continuous-batching server against one launch per request).
+--impl reference runs only the CPU decoder (the reference arm).
 
-Under torchrun every rank decodes its own copy of the batch (weak scaling, no
-data exchange); the step time is the max over ranks.
+Under torchrun every rank decodes its own batch of the same shape (weak
+scaling, no data exchange); the step time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -40,9 +48,12 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     # name: (corpus kind, count, max seconds, chain segment seconds)
     "mixed4096": ("mixed", 4096, 30.0, 1e9),
+    "pareto16384": ("pareto", 16384, 120.0, 1e9),
     "plain64": ("plain64", 64, 1.0, 1.0),
     "long7200": ("long", 1, 7200.0, 1.0),
+    "serve": ("lognormal", 512, 600.0, 1.0),
 }
+METRIC = "audio-sec decoded/sec on 1 B200 (bit-exact)"
 
 
 def log(*a):
@@ -56,8 +67,8 @@ def load_inputs(workload, count=None):
     from oracle.corpus import build_corpus
     kind, n, secs, seg = WORKLOADS[workload]
     t = time.time()
-    paths = build_corpus(kind if kind != "plain64" else "plain64", os.path.join(ROOT, "corpus"),
-                         count=count or n, seconds=secs if kind != "plain64" else None)
+    paths = build_corpus(kind, os.path.join(ROOT, "corpus"), count=count or n,
+                         seconds=secs if kind != "plain64" else None)
     files = [open(p, "rb").read() for p in paths]
     log("corpus %s: %d files, %.1f MB, %.1fs" % (workload, len(files), sum(map(len, files)) / 1e6,
                                                  time.time() - t))
@@ -90,8 +101,7 @@ class DeviceBatch:
             base_p += len(ix.pkt_len)
             self.audio_s += ix.play48 / 48000.0
             self.pcm_bytes += int(ix.play48) * ix.channels * 2
-            # packet bytes decoded, preroll packets included
-            for c in range(len(ix.first)):
+            for c in range(len(ix.first)):   # packet bytes decoded, preroll packets included
                 a, b = int(ix.first[c]), int(ix.first[c]) + int(ix.npkts[c])
                 self.pkt_bytes += int(ix.pkt_len[a:b].sum())
         cat = lambda xs: np.ascontiguousarray(np.concatenate(xs))
@@ -112,7 +122,7 @@ class DeviceBatch:
         self.out = torch.empty(max(tot, 1), dtype=torch.int16, device=dev)
         self.res = torch.zeros(4 * self.n, dtype=torch.int32, device=dev)
 
-    def batch(self, width, schedule, order=None):
+    def batch(self, width, schedule, order=None, block=0, graph=0):
         from cuopus_b200 import cuopus_native as cn
         b = cn.Batch()
         t = self.t
@@ -121,11 +131,15 @@ class DeviceBatch:
         b.trim, b.keep, b.out_off = t["trim"].data_ptr(), t["keep"].data_ptr(), t["out_off"].data_ptr()
         b.out, b.res = self.out.data_ptr(), self.res.data_ptr()
         b.nchains, b.width, b.schedule, b.max_groups = self.n, width, schedule, 0
+        b.block, b.graph = block, graph
         self._order = None
         if order is not None:
             self._order = np.ascontiguousarray(np.asarray(order, np.uint32))
             b.order = self._order.ctypes.data
         return b
+
+    def results(self):
+        return self.res.view(-1, 4).cpu().numpy().view(np.uint32)
 
 
 # ------------------------------------------------------------------ clocks
@@ -184,12 +198,10 @@ def cpu_decode(files, seg, budget_s, threads):
     """libopus on host threads over a prefix of the workload; returns
     (audio-s/s, audio seconds decoded, seconds, files used)."""
     from oracle import ogg_port, ref_decode
-    t_all = time.time()
     audio = 0.0
     used = 0
     elapsed = 0.0
-    # decode in groups so the sample stays bounded by the time budget
-    group = max(threads * 4, 16)
+    group = max(threads * 4, 16)      # decode in groups so the sample stays bounded
     while used < len(files) and elapsed < budget_s:
         chunk = files[used:used + group]
         pk_all, ch_all, chains_all = [], [], []
@@ -198,11 +210,9 @@ def cpu_decode(files, seg, budget_s, threads):
             pk_all.append(ix["packets"])
             ch_all.append(ix["channels"])
             chains_all.append(ogg_port.build_chains(ix, seg, 250.0))
-            audio_f = ix["play48"] / 48000.0
-            audio += audio_f
+            audio += ix["play48"] / 48000.0
         t0 = time.time()
-        # one oracle call per channel count (chains of a call share it)
-        for want_ch in (1, 2):
+        for want_ch in (1, 2):          # one oracle call per channel count
             pk, chains = [], []
             base = 0
             for p, ch, cs in zip(pk_all, ch_all, chains_all):
@@ -218,6 +228,161 @@ def cpu_decode(files, seg, budget_s, threads):
     return audio / elapsed if elapsed > 0 else 0.0, audio, elapsed, used
 
 
+# ------------------------------------------------------------------ helpers
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def profile_traffic():
+    """DRAM bytes per algorithmic byte of the decode kernel, from the committed
+    ncu summary (profiles/k_decode_chains_traffic.json), or None."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "k_decode_chains_traffic.json")))
+        return float(d["dram_bytes"]) / float(d["algorithmic_bytes"])
+    except (OSError, ValueError, KeyError, ZeroDivisionError):
+        return None
+
+
+def timed_steps(cn, b, stream, steps):
+    """K engine calls between two events on the stream; per-call kernel ms."""
+    import torch
+    kern = []
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        kern.append(cn.decode_batch(b, stream.cuda_stream))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, kern
+
+
+def schedule_batch(cn, db, stream, args):
+    """Warm-up work of the scheduled form (untimed): plain form timing, cycle
+    recording, cost model training, autotuning.  Returns (batch, info)."""
+    import torch
+    from cuopus_b200 import costmodel
+    info = {}
+    # plain one-launch form: one warp per chain, index order
+    plain_b = db.batch(32, 2, None, 128, 0)
+    cn.decode_batch(plain_b, stream.cuda_stream)
+    torch.cuda.synchronize()
+    plain_ms, _ = timed_steps(cn, plain_b, stream, max(1, min(args.steps, 2)))
+    info["plain"] = {"ms_per_step": plain_ms, "value": db.audio_s / (plain_ms / 1e3), "width": 32, "block": 128,
+                     "schedule": "plain, index order"}
+    res = db.results()
+    cycles = res[:, 3].astype(np.float64)
+    # learned order (the packet-count order is the fallback)
+    order = costmodel.packet_order(db.cap_pkts, db.chans)
+    info["order"] = "packets x channels"
+    if args.order == "mlp":
+        feats = costmodel.chain_features(plain_b)
+        model = costmodel.CostModel(seed=1)
+        t0 = time.time()
+        losses = model.fit(feats, np.maximum(cycles, 1.0), steps=1500, lr=3e-3)
+        pred = model.predict(feats)
+        y, yh = np.log(np.maximum(cycles, 1.0)), np.log(pred)
+        r2 = 1.0 - np.sum((y - yh) ** 2) / np.sum((y - y.mean()) ** 2)
+        order = np.argsort(-pred, kind="stable")
+        info["order"] = "learned (MLP 16-64-64-1)"
+        info["cost_model"] = {"train_s": round(time.time() - t0, 2), "loss_first": float(losses[0]),
+                              "loss_last": float(losses[-1]), "r2_log_cycles": round(float(r2), 4)}
+    # autotune width x block on the scheduled form
+    width, block = args.width, args.block
+    if not args.no_tune:
+        b = db.batch(32, 1, order, 128, 1)
+        width, block, table = cn.autotune(b, widths=(8, 16, 32), blocks=(64, 128), reps=1,
+                                          stream=stream.cuda_stream)
+        info["autotune"] = {"%dx%d" % k: (round(v, 1) if v else None) for k, v in table.items()}
+    sched = {"queue": 1, "static": 0, "plain": 2}[args.schedule]
+    b = db.batch(width, sched, order if sched == 1 else None, block, 1 if sched != 2 else 0)
+    info.update(width=width, block=block)
+    return b, info
+
+
+# ------------------------------------------------------------------ serving workload
+
+def serve_bench(args, files, dev):
+    """Poisson arrivals through the continuous-batching server, against the
+    plain form that decodes one request per launch in arrival order."""
+    import torch
+    from cuopus_b200 import cuopus_native as cn
+    from cuopus_b200.serving import Server
+    rng = np.random.default_rng(7)
+    n = len(files)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
+    audio = [cn.probe_pcm(f)[0] / 48000.0 for f in files]
+    total_audio = float(sum(audio))
+    out = {}
+    # continuous batching
+    with Server(budget_bytes=args.budget_gb << 30, width=args.width, block=args.block) as srv:
+        srv.wait(srv.submit(files[0]))                      # warm-up (context, slots)
+        ids = [None] * n
+        done_lat = [0.0] * n
+        t0 = time.perf_counter()
+
+        def waiter():
+            for i in range(n):
+                while ids[i] is None:
+                    time.sleep(0.0005)
+                _, _, done_lat[i] = srv.wait(ids[i])
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        for i in range(n):
+            d = arrivals[i] - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            ids[i] = srv.submit(files[i])
+        th.join()
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        lat = np.array(done_lat)
+        out["served"] = {"value": total_audio / wall, "p50_ms": float(np.percentile(lat, 50)),
+                         "p99_ms": float(np.percentile(lat, 99)), "wall_s": wall, "waves": st["waves"],
+                         "wave_chains": st["wave_chains"], "requests": n}
+    # one launch per request, arrival order, one at a time
+    stream = torch.cuda.current_stream()
+    caps = []
+    for f in files:
+        play, ch = cn.probe_pcm(f)
+        caps.append(play * ch)
+    buf = torch.empty(max(caps), dtype=torch.int16, device=dev)
+    host = torch.empty(max(caps), dtype=torch.int16, pin_memory=True)
+    import ctypes
+    lib = cn.lib()
+    err = ctypes.create_string_buffer(512)
+    lat = []
+    t0 = time.perf_counter()
+    for i, f in enumerate(files):
+        d = arrivals[i] - (time.perf_counter() - t0)
+        if d > 0:
+            time.sleep(d)
+        ba = (ctypes.c_char_p * 1)(f)
+        la = (ctypes.c_size_t * 1)(len(f))
+        oa = (ctypes.c_void_p * 1)(buf.data_ptr())
+        ca = (ctypes.c_size_t * 1)(caps[i])
+        ol = (ctypes.c_int64 * 1)()
+        oc = (ctypes.c_int32 * 1)()
+        rc = lib.cuopus_decode_i16_multi(ba, la, 1, oa, ca, ol, oc, ctypes.c_void_p(stream.cuda_stream), err, 512)
+        if rc:
+            raise RuntimeError(err.value.decode())
+        host[:caps[i]].copy_(buf[:caps[i]], non_blocking=True)
+        torch.cuda.synchronize()
+        lat.append((time.perf_counter() - t0 - arrivals[i]) * 1e3)
+    wall = time.perf_counter() - t0
+    lat = np.array(lat)
+    out["one_launch_per_request"] = {"value": total_audio / wall, "p50_ms": float(np.percentile(lat, 50)),
+                                     "p99_ms": float(np.percentile(lat, 99)), "wall_s": wall}
+    out["audio_s"] = total_audio
+    out["arrival_rate_per_s"] = args.rate
+    return out
+
+
 # ------------------------------------------------------------------ main
 
 def main():
@@ -228,10 +393,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed4096", choices=sorted(WORKLOADS))
     ap.add_argument("--count", type=int, default=None, help="override the stream count (development)")
-    ap.add_argument("--width", type=int, default=int(os.environ.get("CUOPUS_STRIDE", "32")))
-    ap.add_argument("--schedule", default="queue", choices=["queue", "static"])
+    ap.add_argument("--width", type=int, default=32, help="lanes per chain when not autotuned")
+    ap.add_argument("--block", type=int, default=128, help="threads per block when not autotuned")
+    ap.add_argument("--schedule", default="queue", choices=["queue", "static", "plain"])
+    ap.add_argument("--order", default="mlp", choices=["mlp", "packets"])
+    ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--rate", type=float, default=100.0, help="serve: Poisson arrivals per second")
+    ap.add_argument("--budget-gb", type=int, default=40, help="serve: admission budget")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -250,13 +420,14 @@ def main():
             if i >= args.warmup:
                 rates.append(r)
         v = statistics.median(rates)
-        line = {"metric": "audio-sec decoded/sec on 1 B200 (bit-exact)", "value": v, "unit": "audio-s/s",
-                "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "int16", "data": "synthetic (seeded, vendored libopus encoder)",
-                "config": {"workload": args.workload, "chains": None, "sample_files": used},
+        line = {"metric": METRIC, "value": v, "unit": "audio-s/s", "impl": "reference", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "int16",
+                "data": "synthetic (seeded, vendored libopus encoder)",
+                "config": {"workload": args.workload, "sample_files": used},
                 "cpu_baseline": {"value": v, "unit": "audio-s/s", "cores": threads, "kind": "reference",
-                                 "sample": "first %d streams (%.0f audio-s) per step" % (used, audio)},
+                                 "sample": "libopus 1.5.2 fixed point, %d host threads, first %d streams "
+                                           "(%.0f audio-s) per step" % (threads, used, audio)},
                 "e2e": {"value": v, "unit": "audio-s/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return 0
@@ -271,39 +442,41 @@ def main():
     from cuopus_b200 import cuopus_native as cn
 
     files, seg = load_inputs(args.workload, args.count)
-    db = DeviceBatch(files, seg, dev)
     cn.warmup()
-    sched = 1 if args.schedule == "queue" else 0
-    order = None
-    if sched == 1:
-        # longest first: packets x channels as the cost proxy
-        order = np.argsort(-(db.cap_pkts.astype(np.int64) * db.chans), kind="stable")
-    b = db.batch(args.width, sched, order)
+
+    if args.workload == "serve":
+        r = serve_bench(args, files, dev)
+        if rank == 0:
+            s = r["served"]
+            line = {"metric": METRIC, "value": s["value"], "unit": "audio-s/s", "n_gpus": world, "steps": 1,
+                    "warmup": 1, "ms_per_step": s["wall_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
+                    "vs_baseline": None, "dtype": "int16", "data": "synthetic (seeded, vendored libopus encoder)",
+                    "config": {"workload": "serve", "requests": s["requests"], "arrivals_per_s": args.rate,
+                               "lengths": "log-normal median 30 s, sigma 1, clipped to [5, 600] s",
+                               "budget_gb": args.budget_gb},
+                    "latency_ms": {"p50": s["p50_ms"], "p99": s["p99_ms"]}, "serve": r}
+            print(json.dumps(line), flush=True)
+        return 0
+
+    db = DeviceBatch(files, seg, dev)
     stream = torch.cuda.current_stream()
+    b, info = schedule_batch(cn, db, stream, args)
+    for _ in range(args.warmup):
+        cn.decode_batch(b, stream.cuda_stream)
+    res = db.results()
+    bad = int((res[:, 0] != 0).sum())
+    if bad:
+        log("WARNING: %d chains stopped with a decode error" % bad)
 
     def barrier():
         if world > 1:
             import torch.distributed as dist
             dist.barrier()
 
-    for _ in range(args.warmup):
-        cn.decode_batch(b, stream.cuda_stream)
-    res = db.res.view(-1, 4).cpu().numpy()
-    bad = int((res[:, 0] != 0).sum())
-    if bad:
-        log("WARNING: %d chains stopped with a decode error" % bad)
     barrier()
     torch.cuda.synchronize()
-    kern = []
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            kern.append(cn.decode_batch(b, stream.cuda_stream))
-        e1.record(stream)
-        torch.cuda.synchronize()
-    step_ms = e0.elapsed_time(e1) / args.steps
+        step_ms, kern = timed_steps(cn, b, stream, args.steps)
     if world > 1:
         import torch.distributed as dist
         t = torch.tensor([step_ms], device=dev)
@@ -313,22 +486,21 @@ def main():
     value = world * db.audio_s / (step_ms / 1e3)
     kern_ms = statistics.mean(kern)
     alg_bytes = db.pkt_bytes + db.pcm_bytes
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except (OSError, ValueError):
-        pass
-    peak = peaks.get("hbm_gbs", 6650.0)
+    pk = peaks()
+    peak = pk.get("hbm_gbs")
+    peak_src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9
+    ratio = profile_traffic()
 
     # e2e through the C ABI from host bytes, PCM read back to pinned host memory
     e2e = None
     if not args.no_e2e:
+        import ctypes
         play = [cn.probe_pcm(f) for f in files]
         caps = [p * c for p, c in play]
         outs = [torch.empty(max(c, 1), dtype=torch.int16, device=dev) for c in caps]
         host = torch.empty(max(sum(caps), 1), dtype=torch.int16, pin_memory=True)
-        import ctypes
         lib = cn.lib()
         n = len(files)
         ba = (ctypes.c_char_p * n)(*files)
@@ -340,6 +512,7 @@ def main():
         err = ctypes.create_string_buffer(512)
         os.environ["CUOPUS_SEG_S"] = str(seg)
         os.environ["CUOPUS_MAX_BATCH"] = str(10 ** 8)
+        os.environ["CUOPUS_STRIDE"] = str(info["width"])
 
         def e2e_step():
             rc = lib.cuopus_decode_i16_multi(ba, la, n, oa, ca, ol, oc, ctypes.c_void_p(stream.cuda_stream),
@@ -369,23 +542,27 @@ def main():
                "ms_per_step": e2e_s * 1e3}
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and args.cpu_budget > 0:
         r, audio, el, used = cpu_decode(files, seg, args.cpu_budget, threads)
         cpu = {"value": r, "unit": "audio-s/s", "cores": threads, "kind": "reference",
                "sample": "libopus 1.5.2 fixed point on %d host threads: first %d of %d streams (%.0f audio-s, %.1fs)"
                          % (threads, used, len(files), audio, el)}
 
     if rank == 0:
-        line = {"metric": "audio-sec decoded/sec on 1 B200 (bit-exact)", "value": value, "unit": "audio-s/s",
-                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16",
-                "data": "synthetic (seeded, vendored libopus encoder)",
+        plain = info.pop("plain")
+        line = {"metric": METRIC, "value": value, "unit": "audio-s/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "int16", "data": "synthetic (seeded, vendored libopus encoder)",
                 "config": {"workload": args.workload, "streams": len(files), "chains": db.n,
-                           "audio_s_per_gpu": round(db.audio_s, 1), "width": args.width,
-                           "schedule": args.schedule, "l2": "inputs and outputs exceed L2 (no flush needed)"},
+                           "audio_s_per_gpu": round(db.audio_s, 1), "schedule": args.schedule, **info,
+                           "l2": "inputs and outputs exceed L2 (no flush needed)"},
+                "plain": {**plain, "value": world * plain["value"], "speedup_of_scheduled": value /
+                          (world * plain["value"])},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": None,
-                             "alg_bytes_per_launch": alg_bytes, "kernel_ms": kern_ms},
+                             "frac": achieved / peak, "peak_source": peak_src,
+                             "traffic": alg_bytes * ratio if ratio else None,
+                             "alg_bytes_per_launch": alg_bytes, "kernel_ms": kern_ms,
+                             "kernel": "k_decode_chains"},
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "gpu_launches": args.steps,
                 "decode_errors": bad}
         print(json.dumps(line), flush=True)

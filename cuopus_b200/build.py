@@ -52,7 +52,7 @@ def _run(cmd):
 
 
 def build_libcuopus(force=False):
-    deps = _sources("libcuopus.cu", "decode_kernel.cu", "costmodel.cu", "kernels.cuh", "ogg_demux.cpp",
+    deps = _sources("libcuopus.cu", "decode_kernel.cu", "costmodel.cu", "server.cu", "kernels.cuh", "ogg_demux.cpp",
                     "ogg_demux.h", "dec") + [os.path.join(ROOT, "include", "cuopus.h")]
     if not force and not _stale(LIBCUOPUS, deps):
         return LIBCUOPUS
@@ -66,10 +66,12 @@ def build_libcuopus(force=False):
                    "-o", os.path.join(obj, "decode_kernel.o")])
     _run(common + ["-Xptxas", "-v", "-c", os.path.join(CSRC, "libcuopus.cu"), "-o", os.path.join(obj, "libcuopus.o")])
     _run(common + ["-Xptxas", "-v", "-c", os.path.join(CSRC, "costmodel.cu"), "-o", os.path.join(obj, "costmodel.o")])
+    _run(common + ["-c", os.path.join(CSRC, "server.cu"), "-o", os.path.join(obj, "server.o")])
     _run(common + ["-c", os.path.join(CSRC, "ogg_demux.cpp"), "-o", os.path.join(obj, "ogg_demux.o")])
     tmp = LIBCUOPUS + ".tmp"
     _run([NVCC, *ARCH, "-shared", "-o", tmp] +
-         [os.path.join(obj, o) for o in ("decode_kernel.o", "libcuopus.o", "costmodel.o", "ogg_demux.o")])
+         [os.path.join(obj, o) for o in ("decode_kernel.o", "libcuopus.o", "costmodel.o", "server.o",
+                                         "ogg_demux.o")])
     os.replace(tmp, LIBCUOPUS)
     return LIBCUOPUS
 

@@ -49,6 +49,10 @@ struct DecodeArgs {
 cudaError_t decode_kernel_occupancy(int block, int *blocks_per_sm);
 cudaError_t decode_kernel_launch(const DecodeArgs &a, int blocks, int block, cudaStream_t st);
 
+// The 48 -> 16 kHz resampler of libcuopus.cu for other host translation units:
+// uploads the taps to the current device on first use, then launches on st.
+cudaError_t resample_into(const int16_t *in, long long avail, long long n_out, float *out, cudaStream_t st);
+
 #ifdef CUO_DECODE_KERNEL_TU
 // Resident 128-thread blocks per SM the register allocation is sized for.
 #ifndef CUO_MIN_BLOCKS
@@ -90,7 +94,9 @@ __global__ void __launch_bounds__(128, CUO_MIN_BLOCKS) k_decode_chains(DecodeArg
 }
 #endif
 
-#ifndef CUO_DECODE_KERNEL_TU
+// The resampler kernel and its taps belong to libcuopus.cu; other host
+// translation units define CUO_NO_RESAMPLE_KERNEL and use resample_into.
+#if !defined(CUO_DECODE_KERNEL_TU) && !defined(CUO_NO_RESAMPLE_KERNEL)
 enum { RS_TAPS = 49, RS_PAD = 24, RS_OUT_PER_THREAD = 4, RS_THREADS = 256,
        RS_TILE_OUT = RS_THREADS * RS_OUT_PER_THREAD, RS_TILE_IN = 3 * RS_TILE_OUT + RS_TAPS - 1 };
 

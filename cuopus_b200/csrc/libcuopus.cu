@@ -180,10 +180,13 @@ void make_taps(float *taps)
     for (int i = 0; i < n; i++) taps[i] = (float)(h[i] / total);
 }
 
+std::mutex g_taps_mu;   // the taps upload is also reached from the server thread
+
 int ensure_taps(cudaStream_t st, Err &err)
 {
     int dev = 0;
     CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_taps_mu);
     if (G.taps_dev == dev) return RC_OK;
     float taps[cuo::RS_TAPS];
     make_taps(taps);
@@ -598,6 +601,15 @@ void record_stats(const Plan &P, bool resampled)
 }
 
 } // namespace
+
+cudaError_t cuo::resample_into(const int16_t *in, long long avail, long long n_out, float *out, cudaStream_t st)
+{
+    Err err(nullptr, 0);
+    int rc = resample(in, avail, n_out, out, st, err);
+    if (rc == RC_OK) return cudaSuccess;
+    cudaError_t e = cudaGetLastError();
+    return e != cudaSuccess ? e : cudaErrorInvalidValue;
+}
 
 // ====================================================================== C ABI
 

@@ -151,6 +151,48 @@ int cuopus_mlp_grad(const float *params_dev, const float *x_dev, const float *t_
 int cuopus_mlp_train(float *params_dev, const float *x_dev, const float *t_dev, int n, int steps, float lr,
                      float *losses, void *cuda_stream, char *errbuf, size_t errcap);
 
+/* ---- Extension: continuous-batching decode server (no counterpart in the
+ * reference, whose daemon decodes one request at a time, decode_cli.cu:572-678).
+ * Requests are demuxed on the submitting thread and admitted, oldest first,
+ * when their packets, PCM and output fit in a device arena of budget_bytes
+ * allocated once at creation; their chains are packed into decode waves of at
+ * most wave_chains chains, up to max_inflight waves in flight on the server's
+ * own streams, so requests that arrive while others decode join the next wave.
+ * The server owns one host thread and max_inflight streams on the device that
+ * is current at creation.  Results are identical to the one-shot entry points
+ * (a fresh decoder per chain).  Return codes as above, plus 4 = timeout. */
+typedef struct cuopus_server cuopus_server;
+typedef struct cuopus_server_config {
+    int64_t budget_bytes;   /* device arena for admitted requests (0 = 40 GiB) */
+    int32_t width;          /* lanes per chain (0 = 32) */
+    int32_t block;          /* threads per block (0 = 128) */
+    int32_t max_inflight;   /* decode waves in flight (0 = 2) */
+    int32_t wave_chains;    /* chains per wave (0 = the resident lane groups of the GPU) */
+    double seg_s;           /* chain length (0 = 1 s) */
+    double preroll_ms;      /* chain preroll (0 = 250 ms) */
+    int32_t f16k;           /* 1: float32 16 kHz output (mono only); 0: int16 48 kHz interleaved */
+} cuopus_server_config;
+typedef struct cuopus_server_stats {
+    int64_t completed, failed, waves, chains, pending, active;
+    int64_t arena_used, arena_bytes, wave_chains;
+    double audio_s;         /* playable audio seconds of completed requests */
+    double wall_ms;         /* first submit to last completion */
+    double p50_ms, p99_ms, max_ms;   /* request latency, submit to completion */
+} cuopus_server_stats;
+
+int cuopus_server_create(const cuopus_server_config *cfg, cuopus_server **out, char *errbuf, size_t errcap);
+/* Queue one Ogg Opus stream; *id identifies it.  RC 1 for a stream that does
+ * not demux (nothing is queued). */
+int cuopus_server_submit(cuopus_server *s, const uint8_t *ogg, size_t n, uint64_t *id, char *errbuf, size_t errcap);
+/* Wait for a request (timeout_ms < 0: forever), copy its output to host_out
+ * (may be NULL) and release it.  out_samples: samples per channel (int16) or
+ * 16 kHz samples (f16k); latency_ms: submit to completion. */
+int cuopus_server_wait(cuopus_server *s, uint64_t id, int64_t timeout_ms, void *host_out, size_t out_cap_bytes,
+                       int64_t *out_samples, int32_t *channels, double *latency_ms, char *errbuf, size_t errcap);
+int cuopus_server_get_stats(cuopus_server *s, cuopus_server_stats *st);
+/* Finish admitted work, drop queued requests, free everything. */
+void cuopus_server_destroy(cuopus_server *s);
+
 /* Extension: fp32 48->16 kHz resample of a device int16 mono stream (the
  * kernel behind the f16k entries): out[i], i < n_out, from in[0..avail). */
 int cuopus_resample48to16(const int16_t *in_dev, int64_t avail, int64_t n_out, float *out_dev, void *cuda_stream,
