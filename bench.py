@@ -122,9 +122,10 @@ class DeviceBatch:
         self.out = torch.empty(max(tot, 1), dtype=torch.int16, device=dev)
         self.res = torch.zeros(4 * self.n, dtype=torch.int32, device=dev)
 
-    def batch(self, width, schedule, order=None, block=0, graph=0):
+    def batch(self, width, schedule, order=None, block=0, graph=0, scalar=0):
         from cuopus_b200 import cuopus_native as cn
         b = cn.Batch()
+        b.scalar = scalar
         t = self.t
         b.data, b.off, b.len = t["blob"].data_ptr(), t["off"].data_ptr(), t["len"].data_ptr()
         b.first, b.npkts, b.channels = t["first"].data_ptr(), t["npkts"].data_ptr(), t["chans"].data_ptr()
@@ -267,13 +268,22 @@ def schedule_batch(cn, db, stream, args):
     import torch
     from cuopus_b200 import costmodel
     info = {}
-    # plain one-launch form: one warp per chain, index order
+    # plain one-launch forms, one warp per chain, index order: the reference
+    # kernel's layout (one lane of the warp decodes) and with the lanes
+    # splitting the independent loops
+    reps = max(1, min(args.steps, 2))
+    plain_ref = db.batch(32, 2, None, 128, 0, scalar=1)
+    cn.decode_batch(plain_ref, stream.cuda_stream)
+    torch.cuda.synchronize()
+    ref_ms, _ = timed_steps(cn, plain_ref, stream, reps)
     plain_b = db.batch(32, 2, None, 128, 0)
     cn.decode_batch(plain_b, stream.cuda_stream)
     torch.cuda.synchronize()
-    plain_ms, _ = timed_steps(cn, plain_b, stream, max(1, min(args.steps, 2)))
-    info["plain"] = {"ms_per_step": plain_ms, "value": db.audio_s / (plain_ms / 1e3), "width": 32, "block": 128,
-                     "schedule": "plain, index order"}
+    plain_ms, _ = timed_steps(cn, plain_b, stream, reps)
+    info["plain"] = {"ms_per_step": ref_ms, "value": db.audio_s / (ref_ms / 1e3), "width": 32, "block": 128,
+                     "schedule": "plain one-launch, one warp per chain, one lane decoding, index order",
+                     "lane_split": {"ms_per_step": plain_ms, "value": db.audio_s / (plain_ms / 1e3),
+                                    "schedule": "plain one-launch, one warp per chain, 32 lanes, index order"}}
     res = db.results()
     cycles = res[:, 3].astype(np.float64)
     # learned order (the packet-count order is the fallback)
@@ -557,7 +567,8 @@ def main():
                            "audio_s_per_gpu": round(db.audio_s, 1), "schedule": args.schedule, **info,
                            "l2": "inputs and outputs exceed L2 (no flush needed)"},
                 "plain": {**plain, "value": world * plain["value"], "speedup_of_scheduled": value /
-                          (world * plain["value"])},
+                          (world * plain["value"]),
+                          "speedup_of_scheduled_over_lane_split": value / (world * plain["lane_split"]["value"])},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_source": peak_src,
                              "traffic": alg_bytes * ratio if ratio else None,

@@ -25,6 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 LIBCUOPUS = os.path.join(LIB, "libcuopus.so")
 HOSTCHECK = os.path.join(LIB, "libcuopus_hostcheck.so")
+HOSTCHECK_REV = os.path.join(LIB, "libcuopus_hostcheck_rev.so")
 CLI = os.path.join(BIN, "cuopus_decode")
 
 
@@ -77,14 +78,17 @@ def build_libcuopus(force=False):
 
 
 def build_hostcheck(force=False):
+    """The host build, and a second one whose lane-split loops run backwards
+    (a test that their iterations are independent)."""
     deps = _sources("hostcheck.cpp", "dec")
-    if not force and not _stale(HOSTCHECK, deps):
-        return HOSTCHECK
-    os.makedirs(LIB, exist_ok=True)
-    tmp = HOSTCHECK + ".tmp"
-    _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-w", "-I", CSRC,
-          os.path.join(CSRC, "hostcheck.cpp"), "-o", tmp, "-lpthread"])
-    os.replace(tmp, HOSTCHECK)
+    for target, extra in ((HOSTCHECK, []), (HOSTCHECK_REV, ["-DCUO_LFOR_REVERSE"])):
+        if not force and not _stale(target, deps):
+            continue
+        os.makedirs(LIB, exist_ok=True)
+        tmp = target + ".tmp"
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-w", "-I", CSRC, *extra,
+              os.path.join(CSRC, "hostcheck.cpp"), "-o", tmp, "-lpthread"])
+        os.replace(tmp, target)
     return HOSTCHECK
 
 

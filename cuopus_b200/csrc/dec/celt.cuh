@@ -382,6 +382,68 @@ DNI void comb_filter(int32_t *y, int32_t *x, int T0, int T1, int N, int16_t g0, 
     }
 }
 
+// comb_filter split across the lanes.  In place (y == x) output i reads the
+// input at i and outputs at i - T - 2 .. i - T + 2 (T >= 15), so a block of
+// min(T0, T1) - 2 consecutive outputs depends only on earlier blocks: the
+// blocks run in order with a barrier between them and the outputs of a block
+// in parallel, each with the serial code's exact arithmetic.  Out of place
+// every output depends on the input only and one block covers the frame.
+DNI void comb_filter_lanes(Lanes L, int32_t *y, int32_t *x, int T0, int T1, int N, int16_t g0, int16_t g1,
+                           int tapset0, int tapset1, const int16_t *window, int overlap)
+{
+    const int16_t gains[3][3] = {{10048, 7112, 4248}, {15200, 8784, 0}, {26208, 3280, 0}};
+    lsync(L);
+    if (g0 == 0 && g1 == 0) {
+        if (x != y) {
+            LFOR(L, i, 0, N) y[i] = x[i];
+            lsync(L);
+        }
+        return;
+    }
+    T0 = imax(T0, 15);
+    T1 = imax(T1, 15);
+    int16_t g00 = (int16_t)c_mul16_p15(g0, gains[tapset0][0]);
+    int16_t g01 = (int16_t)c_mul16_p15(g0, gains[tapset0][1]);
+    int16_t g02 = (int16_t)c_mul16_p15(g0, gains[tapset0][2]);
+    int16_t g10 = (int16_t)c_mul16_p15(g1, gains[tapset1][0]);
+    int16_t g11 = (int16_t)c_mul16_p15(g1, gains[tapset1][1]);
+    int16_t g12 = (int16_t)c_mul16_p15(g1, gains[tapset1][2]);
+    if (g0 == g1 && T0 == T1 && tapset0 == tapset1) overlap = 0;
+    const int B = x == y ? imin(T0, T1) - 2 : imax(N, 1);
+    for (int s = 0; s < overlap; s += B) {
+        int e = imin(s + B, overlap);
+        LFOR(L, i, s, e) {
+            int16_t f = (int16_t)c_mul16_q15(window[i], window[i]);
+            int32_t v = x[i];
+            v = wadd(v, c_mul16_32_q15((int16_t)c_mul16_q15(32767 - f, g00), x[i - T0]));
+            v = wadd(v, c_mul16_32_q15((int16_t)c_mul16_q15(32767 - f, g01), wadd(x[i - T0 + 1], x[i - T0 - 1])));
+            v = wadd(v, c_mul16_32_q15((int16_t)c_mul16_q15(32767 - f, g02), wadd(x[i - T0 + 2], x[i - T0 - 2])));
+            v = wadd(v, c_mul16_32_q15((int16_t)c_mul16_q15(f, g10), x[i - T1]));
+            v = wadd(v, c_mul16_32_q15((int16_t)c_mul16_q15(f, g11), wadd(x[i - T1 + 1], x[i - T1 - 1])));
+            v = wadd(v, c_mul16_32_q15((int16_t)c_mul16_q15(f, g12), wadd(x[i - T1 + 2], x[i - T1 - 2])));
+            y[i] = c_sat(v, CELT_SIG_SAT);
+        }
+        lsync(L);
+    }
+    if (g1 == 0) {
+        if (x != y) {
+            LFOR(L, k, overlap, N) y[k] = x[k];
+            lsync(L);
+        }
+        return;
+    }
+    for (int s = overlap; s < N; s += B) {
+        int e = imin(s + B, N);
+        LFOR(L, k, s, e) {
+            int32_t v = wadd(wadd(wadd(x[k], c_mul16_32_q15(g10, x[k - T1])),
+                                  c_mul16_32_q15(g11, wadd(x[k - T1 + 1], x[k - T1 - 1]))),
+                             c_mul16_32_q15(g12, wadd(x[k - T1 + 2], x[k - T1 - 2])));
+            y[k] = c_sat(v, CELT_SIG_SAT);
+        }
+        lsync(L);
+    }
+}
+
 // celt/celt_decoder.c deemphasis (downsample 1): one-pole recursion, serial
 DNI void deemphasis(Lanes L, int32_t *in0, int32_t *in1, int16_t *pcm, int N, int C, int32_t *mem,
                     int accum)
@@ -1789,11 +1851,7 @@ DNI void celt_decode_lost(Lanes L, CeltDec *st, int N, int LM, CeltScratch *w)
         int end = st->end;
         int effEnd = imax(start, imin(end, T_CELT_EFFEBANDS));
         int16_t *X = w->X;
-        for (int c = 0; c < C; c++) {
-            int32_t *dm = st->decode_mem[c];
-            for (int i = 0; i < CELT_DEC_BUF - N + CELT_OVERLAP; i++) dm[i] = dm[i + N];
-        }
-        lsync(L);
+        for (int c = 0; c < C; c++) lshift_copy(L, st->decode_mem[c], CELT_DEC_BUF - N + CELT_OVERLAP, N);
         if (st->prefilter_and_fold) prefilter_and_fold(st, N, w);
         int16_t decay = loss_duration == 0 ? 1536 : 512;   // QCONST16(1.5f / .5f, DB_SHIFT)
         for (int c = 0; c < C; c++)
@@ -2050,11 +2108,7 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
     int codedBands = clt_compute_allocation(start, end, offsets, cap, alloc_trim, &intensity, &dual_stereo, bits,
                                             &balance, pulses, fine_quant, fine_priority, C, LM, dec);
     unquant_fine_energy(start, end, oldBandE, fine_quant, dec, C);
-    for (int c = 0; c < CC; c++) {
-        int32_t *dm = st->decode_mem[c];
-        for (int i = 0; i < CELT_DEC_BUF - N + CELT_OVERLAP; i++) dm[i] = dm[i + N];
-    }
-    lsync(L);
+    for (int c = 0; c < CC; c++) lshift_copy(L, st->decode_mem[c], CELT_DEC_BUF - N + CELT_OVERLAP, N);
     int16_t *X = w->X;
     quant_all_bands_dec(L, start, end, X, C == 2 ? X + N : 0, w->collapse_masks, pulses, shortBlocks,
                         spread_decision, dual_stereo, intensity, tf_res, len * (8 << 3) - anti_collapse_rsv,
@@ -2072,11 +2126,11 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
     for (int c = 0; c < CC; c++) {
         st->postfilter_period = imax(st->postfilter_period, 15);
         st->postfilter_period_old = imax(st->postfilter_period_old, 15);
-        comb_filter(out_syn[c], out_syn[c], st->postfilter_period_old, st->postfilter_period, T_CELT_SHORTMDCT,
+        comb_filter_lanes(L, out_syn[c], out_syn[c], st->postfilter_period_old, st->postfilter_period, T_CELT_SHORTMDCT,
                     (int16_t)st->postfilter_gain_old, (int16_t)st->postfilter_gain, st->postfilter_tapset_old,
                     st->postfilter_tapset, T_celt_window, CELT_OVERLAP);
         if (LM != 0)
-            comb_filter(out_syn[c] + T_CELT_SHORTMDCT, out_syn[c] + T_CELT_SHORTMDCT, st->postfilter_period,
+            comb_filter_lanes(L, out_syn[c] + T_CELT_SHORTMDCT, out_syn[c] + T_CELT_SHORTMDCT, st->postfilter_period,
                         postfilter_pitch, N - T_CELT_SHORTMDCT, (int16_t)st->postfilter_gain, postfilter_gain,
                         st->postfilter_tapset, postfilter_tapset, T_celt_window, CELT_OVERLAP);
     }

@@ -11,6 +11,120 @@
 
 namespace cuo {
 
+// ------------------------------------------------------------------ packet staging
+//
+// On the device each lane group stages its packets in shared memory with TMA
+// bulk copies (cp.async.bulk global -> shared, completion on an mbarrier),
+// double-buffered: packet k+1 is in flight while packet k is decoded, so the
+// range decoder reads its bytes from shared memory.  Only bytes inside the
+// packet are read from global memory: the 16-byte-aligned interior goes by
+// TMA, the unaligned head and tail (< 16 bytes each) by plain lane loads, and
+// byte a of the packet lands at buf + (a mod 16) so both sides of the copy
+// stay 16-byte aligned.  Packets longer than a buffer are read in place.
+// Every wait is bounded: if a copy does not complete in time the group stops
+// staging (decoding continues from global memory, with the same result) and
+// waits, again bounded, for its copies in flight before the chain returns.
+enum { STAGE_BUF = 1536, STAGE_BYTES = 2 * STAGE_BUF + 32 };   // per group: 2 buffers + 2 mbarriers
+
+struct PacketStage {
+    uint8_t *buf;        // 2 x STAGE_BUF bytes of shared memory, or null (host build / disabled)
+    uint64_t *bar;       // 2 mbarriers
+    unsigned parity;     // bit b: phase parity the next wait on buffer b expects
+    unsigned pending;    // bit b: a TMA copy into buffer b was issued and not yet waited for
+    int ok;              // staging usable (0 after a timed-out wait)
+};
+
+#ifdef __CUDACC__
+DFN uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+DFN void stage_init(const Lanes &L, PacketStage &S, uint8_t *region)
+{
+    S.buf = region;
+    S.bar = (uint64_t *)(region + 2 * STAGE_BUF);
+    S.parity = 0;
+    S.pending = 0;
+    S.ok = 1;
+    if (L.id == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.bar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.bar[1])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    lsync(L);
+}
+
+// Bounded wait for the completion of buffer b's copy; false on timeout.
+DFN bool stage_wait(PacketStage &S, int b)
+{
+    uint32_t addr = smem_u32(&S.bar[b]), par = (S.parity >> b) & 1u;
+    for (int it = 0; it < (1 << 20); it++) {
+        uint32_t done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(done)
+                     : "r"(addr), "r"(par)
+                     : "memory");
+        if (done) {
+            S.parity ^= 1u << b;
+            S.pending &= ~(1u << b);
+            return true;
+        }
+    }
+    return false;
+}
+
+// Start staging packet (src, n) into buffer b.  Returns false when the packet
+// is read in place instead (too long, staging off).
+DFN bool stage_issue(const Lanes &L, PacketStage &S, int b, const uint8_t *src, int n)
+{
+    if (!S.ok || n <= 0 || n > STAGE_BUF - 32) return false;
+    uintptr_t a = (uintptr_t)src;
+    uintptr_t lo = (a + 15) & ~(uintptr_t)15;         // first aligned byte inside the packet
+    uintptr_t hi = (a + (uintptr_t)n) & ~(uintptr_t)15;   // end of the aligned interior
+    uint8_t *dst = S.buf + b * STAGE_BUF + (a & 15);     // packet byte a at buf + (a mod 16)
+    if (hi > lo) {
+        if (L.id == 0) {
+            uint32_t bytes = (uint32_t)(hi - lo);
+            uint32_t bar = smem_u32(&S.bar[b]);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                             smem_u32(dst + (lo - a))),
+                         "l"((const void *)lo), "r"(bytes), "r"(bar)
+                         : "memory");
+        }
+        S.pending |= 1u << b;
+    } else {
+        lo = hi = a + (uintptr_t)n;                  // no aligned interior: all bytes by lanes
+    }
+    int head = (int)(lo - a), tail0 = (int)(hi - a);
+    LFOR(L, i, 0, head) dst[i] = src[i];
+    LFOR(L, i, tail0, n) dst[i] = src[i];
+    return true;
+}
+
+// Wait for buffer b (issued by stage_issue); false when staging gave up.  The
+// lanes agree on the outcome, so a timeout switches the whole group to
+// in-place reads.
+DFN bool stage_ready(const Lanes &L, PacketStage &S, int b)
+{
+    bool ok = true;
+    if (S.pending & (1u << b)) ok = stage_wait(S, b);
+    ok = __all_sync(L.mask, ok);
+    if (!ok) S.ok = 0;
+    return ok;
+}
+
+// Before the group's region is reused or the kernel returns: let every copy in
+// flight land (bounded).
+DFN void stage_drain(const Lanes &L, PacketStage &S)
+{
+    bool ok = true;
+    for (int b = 0; b < 2; b++)
+        if (S.pending & (1u << b)) ok = stage_wait(S, b) && ok;
+    if (!__all_sync(L.mask, ok)) S.ok = 0;
+}
+#endif
+
 struct ChainResult {
     int32_t stop;          // 0, or the first negative opus_decode return
     uint32_t samples;      // samples per channel decoded
@@ -46,9 +160,11 @@ struct KeepWindow {
 
 // Decode one chain.  pkt_nsamp / pkt_rng (optional) receive per-packet sample
 // counts and final ranges; `out` may be null (decode only).
+// `stage` (device only, may be null) stages the packets in shared memory.
 DNI void decode_chain(Lanes L, ChainSlot *slot, const uint8_t *data, const uint64_t *off,
                       const uint32_t *len, uint32_t first, uint32_t npkts, int channels, int16_t *out,
-                      uint64_t trim, uint64_t keep, uint32_t *pkt_nsamp, uint32_t *pkt_rng, ChainResult *res)
+                      uint64_t trim, uint64_t keep, uint32_t *pkt_nsamp, uint32_t *pkt_rng, ChainResult *res,
+                      PacketStage *stage)
 {
     OpusDec *st = &slot->dec;
     opus_init(st, channels);
@@ -61,9 +177,25 @@ DNI void decode_chain(Lanes L, ChainSlot *slot, const uint8_t *data, const uint6
     win.trim = out ? trim : 0;
     win.keep = out ? keep : 0;
     int32_t stop = 0;
+#ifdef __CUDA_ARCH__
+    bool next_staged = false;
+    if (stage && npkts > 0) next_staged = stage_issue(L, *stage, 0, data + off[first], (int)len[first]);
+#else
+    (void)stage;
+#endif
     for (uint32_t k = 0; k < npkts; k++) {
         uint64_t p = (uint64_t)first + k;
-        int ret = opus_decode_packet(L, st, data + off[p], (int32_t)len[p], slot->frame_buf, &slot->scratch, win);
+        const uint8_t *pk = data + off[p];
+#ifdef __CUDA_ARCH__
+        if (stage) {
+            int b = (int)(k & 1u);
+            bool cur = next_staged;
+            next_staged = k + 1 < npkts && stage_issue(L, *stage, b ^ 1, data + off[p + 1], (int)len[p + 1]);
+            if (cur && stage_ready(L, *stage, b)) pk = stage->buf + b * STAGE_BUF + ((uintptr_t)pk & 15);
+        }
+#endif
+        int ret = opus_decode_packet(L, st, pk, (int32_t)len[p], slot->frame_buf, &slot->scratch, win);
+        lsync(L);   // every lane is done with this packet's buffer before it is refilled
         if (ret < 0) {
             stop = ret;
             if (L.id == 0) {
@@ -77,6 +209,9 @@ DNI void decode_chain(Lanes L, ChainSlot *slot, const uint8_t *data, const uint6
             if (pkt_rng) pkt_rng[k] = st->rangeFinal;
         }
     }
+#ifdef __CUDA_ARCH__
+    if (stage) stage_drain(L, *stage);
+#endif
     if (L.id == 0) {
         res->stop = stop;
         res->samples = (uint32_t)win.pos;

@@ -57,8 +57,29 @@ DFN void lsync(const Lanes &L)
 #endif
 }
 
-// for (i = start; i < end; i++) split across the lanes of the group
+// for (i = start; i < end; i++) split across the lanes of the group.  The
+// iterations of an LFOR loop must not depend on each other; a host test build
+// (CUO_LFOR_REVERSE) runs them in reverse order to check that they do not.
+#ifdef CUO_LFOR_REVERSE
+#define LFOR(L, i, start, end) for (int i = (end) - 1 - (L).id; i >= (start); i -= (L).n)
+#else
 #define LFOR(L, i, start, end) for (int i = (start) + (L).id; i < (end); i += (L).n)
+#endif
+
+// buf[i] = buf[i + shift] for i = 0 .. n-1 (the forward in-place copy that
+// drops the oldest `shift` samples of a history buffer), split across the
+// lanes.  Positions go in blocks of `shift`: block k reads only block k+1,
+// which no lane writes before the barrier that ends block k, so the result is
+// the serial copy's.
+template <class T> DFN void lshift_copy(const Lanes &L, T *buf, int n, int shift)
+{
+    lsync(L);
+    for (int b = 0; b < n; b += shift) {
+        int e = b + shift < n ? b + shift : n;
+        LFOR(L, i, b, e) buf[i] = buf[i + shift];
+        lsync(L);
+    }
+}
 
 // ------------------------------------------------------------------ basic ops
 

@@ -858,7 +858,7 @@ DNI void silk_decode_core(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *xq, con
                           SilkScratch *w)
 {
     int16_t *sLTP = w->sLTP;
-    int32_t *sLTP_Q15 = w->sLTP_Q15, *sLPC_Q14 = w->sLPC_Q14;
+    int32_t *sLTP_Q15 = w->sLTP_Q15;
     const SilkIndices *ix = &c->indices;
     int32_t offset_Q10 = T_silk_Quantization_Offsets_Q10[(ix->signalType >> 1) * 2 + ix->quantOffsetType];
     int NLSF_interpolation_flag = ix->NLSFInterpCoef_Q2 < 4;
@@ -875,7 +875,10 @@ DNI void silk_decode_core(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *xq, con
         c->exc_Q14[i] = e;
         rand_seed = wadd(rand_seed, pulses[i]);
     }
-    for (int i = 0; i < 16; i++) sLPC_Q14[i] = c->sLPC_Q14_buf[i];
+    // LPC synthesis history: the last 16 outputs, in registers (win[15] newest)
+    int32_t win[16];
+#pragma unroll
+    for (int t = 0; t < 16; t++) win[t] = c->sLPC_Q14_buf[t];
     const int32_t *pexc = c->exc_Q14;
     int16_t *pxq = xq;
     int sLTP_buf_idx = c->ltp_mem_length;
@@ -892,7 +895,8 @@ DNI void silk_decode_core(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *xq, con
         int32_t gain_adj_Q16;
         if (ctrl->Gains_Q16[k] != c->prev_gain_Q16) {
             gain_adj_Q16 = s_div32_varq(c->prev_gain_Q16, ctrl->Gains_Q16[k], 16);
-            for (int i = 0; i < 16; i++) sLPC_Q14[i] = s_smulww(gain_adj_Q16, sLPC_Q14[i]);
+#pragma unroll
+            for (int t = 0; t < 16; t++) win[t] = s_smulww(gain_adj_Q16, win[t]);
         } else {
             gain_adj_Q16 = 1 << 16;
         }
@@ -925,17 +929,25 @@ DNI void silk_decode_core(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *xq, con
         }
         int32_t *res = w->res_Q14;
         if (signalType == SIG_VOICED) {
-            // the 5-tap LTP reads lag-2 samples back: serial only across that distance
+            // the 5-tap LTP reads samples at least lag - 2 back, so blocks of
+            // lag - 2 outputs depend only on earlier blocks: lanes split a
+            // block, blocks run in order
             const int32_t *pl = &sLTP_Q15[sLTP_buf_idx - lag + 2];
-            for (int i = 0; i < c->subfr_length; i++) {
-                int32_t p = 2;
-                p = s_smlawb(p, pl[i], B_Q14[0]);
-                p = s_smlawb(p, pl[i - 1], B_Q14[1]);
-                p = s_smlawb(p, pl[i - 2], B_Q14[2]);
-                p = s_smlawb(p, pl[i - 3], B_Q14[3]);
-                p = s_smlawb(p, pl[i - 4], B_Q14[4]);
-                res[i] = wadd(pexc[i], shl32(p, 1));
-                sLTP_Q15[sLTP_buf_idx + i] = shl32(res[i], 1);
+            const int blk = imax(lag - 2, 1);   // lag >= 16 in a valid stream
+            for (int s0 = 0; s0 < c->subfr_length; s0 += blk) {
+                int e0 = imin(s0 + blk, c->subfr_length);
+                LFOR(L, i, s0, e0) {
+                    int32_t p = 2;
+                    p = s_smlawb(p, pl[i], B_Q14[0]);
+                    p = s_smlawb(p, pl[i - 1], B_Q14[1]);
+                    p = s_smlawb(p, pl[i - 2], B_Q14[2]);
+                    p = s_smlawb(p, pl[i - 3], B_Q14[3]);
+                    p = s_smlawb(p, pl[i - 4], B_Q14[4]);
+                    int32_t r = wadd(pexc[i], shl32(p, 1));
+                    res[i] = r;
+                    sLTP_Q15[sLTP_buf_idx + i] = shl32(r, 1);
+                }
+                lsync(L);
             }
             sLTP_buf_idx += c->subfr_length;
             pres = res;
@@ -943,18 +955,24 @@ DNI void silk_decode_core(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *xq, con
             pres = pexc;
         }
         // LPC synthesis: order-10/16 recursion per sample
+        const int order = c->LPC_order;
         for (int i = 0; i < c->subfr_length; i++) {
-            int32_t p = c->LPC_order >> 1;
-            const int32_t *s = &sLPC_Q14[16 + i];
-            for (int j = 0; j < c->LPC_order; j++) p = s_smlawb(p, s[-j - 1], A_Q12[j]);
-            sLPC_Q14[16 + i] = s_add_sat32(pres[i], s_lshift_sat32(p, 4));
-            pxq[i] = (int16_t)s_sat16(s_rshift_round(s_smulww(sLPC_Q14[16 + i], Gain_Q10), 8));
+            int32_t p = order >> 1;
+#pragma unroll
+            for (int j = 0; j < 16; j++)
+                if (j < order) p = s_smlawb(p, win[15 - j], A_Q12[j]);
+            int32_t v = s_add_sat32(pres[i], s_lshift_sat32(p, 4));
+#pragma unroll
+            for (int t = 0; t < 15; t++) win[t] = win[t + 1];
+            win[15] = v;
+            pxq[i] = (int16_t)s_sat16(s_rshift_round(s_smulww(v, Gain_Q10), 8));
         }
-        for (int i = 0; i < 16; i++) sLPC_Q14[i] = sLPC_Q14[c->subfr_length + i];
         pexc += c->subfr_length;
         pxq += c->subfr_length;
     }
-    for (int i = 0; i < 16; i++) c->sLPC_Q14_buf[i] = sLPC_Q14[i];
+    lsync(L);
+#pragma unroll
+    for (int t = 0; t < 16; t++) c->sLPC_Q14_buf[t] = win[t];
     lsync(L);
 }
 
@@ -1219,8 +1237,7 @@ DNI void silk_decode_frame(Lanes L, SilkChan *c, RangeDec *rd, int16_t *pOut, in
         silk_decode_parameters(c, ctrl, condCoding);
         silk_decode_core(L, c, ctrl, pOut, pulses, w);
         int mv = c->ltp_mem_length - c->frame_length;
-        for (int i = 0; i < mv; i++) c->outBuf[i] = c->outBuf[c->frame_length + i];
-        lsync(L);
+        lshift_copy(L, c->outBuf, mv, c->frame_length);
         LFOR(L, i, 0, c->frame_length) c->outBuf[mv + i] = pOut[i];
         lsync(L);
         silk_plc(L, c, ctrl, pOut, 0, w);
@@ -1230,8 +1247,7 @@ DNI void silk_decode_frame(Lanes L, SilkChan *c, RangeDec *rd, int16_t *pOut, in
     } else {
         silk_plc(L, c, ctrl, pOut, 1, w);
         int mv = c->ltp_mem_length - c->frame_length;
-        for (int i = 0; i < mv; i++) c->outBuf[i] = c->outBuf[c->frame_length + i];
-        lsync(L);
+        lshift_copy(L, c->outBuf, mv, c->frame_length);
         LFOR(L, i, 0, c->frame_length) c->outBuf[mv + i] = pOut[i];
         lsync(L);
     }

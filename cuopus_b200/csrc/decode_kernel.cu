@@ -17,14 +17,18 @@
 
 namespace cuo {
 
-cudaError_t decode_kernel_occupancy(int block, int *blocks_per_sm)
+cudaError_t decode_kernel_occupancy(int block, int width, int *blocks_per_sm)
 {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_decode_chains, block, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_decode_chains, block,
+                                                         (size_t)stage_smem_bytes(block, width));
 }
 
 cudaError_t decode_kernel_launch(const DecodeArgs &a, int blocks, int block, cudaStream_t st)
 {
-    k_decode_chains<<<blocks, block, 0, st>>>(a);
+    DecodeArgs b = a;
+    int smem = stage_smem_bytes(block, a.width);
+    b.stage = smem > 0;
+    k_decode_chains<<<blocks, block, (size_t)smem, st>>>(b);
     return cudaGetLastError();
 }
 

@@ -47,7 +47,7 @@ static void *hc_worker(void *arg)
         cuo::decode_chain(L, slot, j->data, j->off, j->len, j->first[c], j->npkts[c], j->channels[c],
                           j->pcm ? j->pcm + j->pcm_off[c] : nullptr, j->trim ? j->trim[c] : 0,
                           j->keep ? j->keep[c] : (uint64_t)-1 / 4, j->pkt_nsamp ? j->pkt_nsamp + r : nullptr,
-                          j->pkt_rng ? j->pkt_rng + r : nullptr, &j->res[c]);
+                          j->pkt_rng ? j->pkt_rng + r : nullptr, &j->res[c], nullptr);
     }
     free(slot);
     return nullptr;

@@ -42,11 +42,22 @@ struct DecodeArgs {
     int nchains;
     int width;                  // lanes per chain: 1, 2, 4, 8, 16 or 32
     int use_queue;
+    int stage;                  // packets staged in shared memory (STAGE_BYTES per group)
+    int scalar;                 // one active lane per group (the reference kernel's slot layout)
 };
 
+// Shared memory a block of `block` threads at `width` lanes per chain uses for
+// packet staging; 0 (no staging) when it would exceed 48 KB per block.
+inline int stage_smem_bytes(int block, int width)
+{
+    int bytes = (block / width) * (int)STAGE_BYTES;
+    return bytes <= 48 * 1024 ? bytes : 0;
+}
+
 // Decoder kernel: defined in decode_kernel.cu, which is compiled on its own
-// (see the note there); the host side reaches it through these two calls.
-cudaError_t decode_kernel_occupancy(int block, int *blocks_per_sm);
+// (see the note there); the host side reaches it through these calls.  The
+// launch decides packet staging from block and width (stage_smem_bytes).
+cudaError_t decode_kernel_occupancy(int block, int width, int *blocks_per_sm);
 cudaError_t decode_kernel_launch(const DecodeArgs &a, int blocks, int block, cudaStream_t st);
 
 // The 48 -> 16 kHz resampler of libcuopus.cu for other host translation units:
@@ -67,10 +78,22 @@ __global__ void __launch_bounds__(128, CUO_MIN_BLOCKS) k_decode_chains(DecodeArg
     L.id = lane - sub * W;
     L.n = W;
     L.mask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << (sub * W));
+    if (a.scalar) {            // the group's first lane decodes alone; the others idle
+        if (L.id != 0) return;
+        L.n = 1;
+        L.mask = 1u << lane;
+    }
     const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int group = (int)(gtid / W);
     const int ngroups = (int)((long long)gridDim.x * blockDim.x / W);
     ChainSlot *slot = a.slots + group;
+    extern __shared__ __align__(16) uint8_t s_stage[];
+    PacketStage S;
+    PacketStage *stage = nullptr;
+    if (a.stage) {
+        stage_init(L, S, s_stage + (size_t)(threadIdx.x / W) * STAGE_BYTES);
+        stage = &S;
+    }
     for (int it = 0; it < a.nchains; it++) {
         int pos;
         if (a.use_queue) {
@@ -87,7 +110,7 @@ __global__ void __launch_bounds__(128, CUO_MIN_BLOCKS) k_decode_chains(DecodeArg
         decode_chain(L, slot, a.data, a.off, a.len, a.first[c], a.npkts[c], a.channels[c],
                      a.out ? a.out + a.out_off[c] : nullptr, a.trim[c], a.keep[c],
                      a.pkt_nsamp ? a.pkt_nsamp + a.rec_off[c] : nullptr,
-                     a.pkt_rng ? a.pkt_rng + a.rec_off[c] : nullptr, &a.res[c]);
+                     a.pkt_rng ? a.pkt_rng + a.rec_off[c] : nullptr, &a.res[c], stage);
         long long t1 = clock64();
         if (L.id == 0) a.res[c].cycles = (uint32_t)min(t1 - t0, 0xffffffffLL);
     }

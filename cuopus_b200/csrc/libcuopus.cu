@@ -77,7 +77,7 @@ struct State {
     long long dev_bytes = 0;
     int taps_dev = -1;
     int occ_dev = -1, occ_blocks = 0, sm_count = 0;
-    int occ_by_warps[5] = {0, 1, 1, 1, 1};       // resident blocks per SM by warps per block
+    int occ[5][6] = {};                          // resident blocks per SM by [warps per block][log2 width]
     // decode launch captured as a CUDA graph (queue reset + kernel) and its key
     cudaGraphExec_t gexec = nullptr;
     cudaStream_t cap_stream = nullptr;
@@ -204,12 +204,13 @@ int ensure_occupancy(Err &err)
     CK(cudaGetDevice(&dev));
     if (G.occ_dev == dev) return RC_OK;
     CK(cudaDeviceGetAttribute(&G.sm_count, cudaDevAttrMultiProcessorCount, dev));
-    for (int w = 1; w <= 4; w++) {
-        int nb = 0;
-        CK(cuo::decode_kernel_occupancy(32 * w, &nb));
-        G.occ_by_warps[w] = nb < 1 ? 1 : nb;
-    }
-    G.occ_blocks = G.occ_by_warps[BLOCK / 32];
+    for (int w = 1; w <= 4; w++)
+        for (int lw = 0; lw <= 5; lw++) {
+            int nb = 0;
+            CK(cuo::decode_kernel_occupancy(32 * w, 1 << lw, &nb));
+            G.occ[w][lw] = nb < 1 ? 1 : nb;
+        }
+    G.occ_blocks = G.occ[BLOCK / 32][5];
     G.occ_dev = dev;
     return RC_OK;
 }
@@ -223,7 +224,9 @@ int block_threads(const cuopus_batch *b)
 // Decoder groups resident on the whole GPU for a block size and width.
 long long resident_groups(int block, int width)
 {
-    return (long long)G.sm_count * G.occ_by_warps[block / 32] * (block / width);
+    int lw = 0;
+    while ((1 << lw) < width) lw++;
+    return (long long)G.sm_count * G.occ[block / 32][lw] * (block / width);
 }
 
 int ensure_events(Err &err)
@@ -355,6 +358,7 @@ int decode_batch(const cuopus_batch *b, cudaStream_t st, float *kernel_ms, Err &
     a.nchains = b->nchains;
     a.width = width;
     a.use_queue = b->schedule == 1;
+    a.scalar = b->scalar != 0;
     CK(cudaEventRecord(G.ev0, st));
     if (b->graph) {
         if ((rc = launch_graph(a, blocks, block, st, err))) return rc;

@@ -476,7 +476,7 @@ extern "C" int cuopus_server_create(const cuopus_server_config *cfg, cuopus_serv
     if (e != cudaSuccess) return fail(errbuf, errcap, 2, "cudaGetDevice: %s", cudaGetErrorString(e));
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->dev);
-    e = cuo::decode_kernel_occupancy(s->block, &per_sm);
+    e = cuo::decode_kernel_occupancy(s->block, s->width, &per_sm);
     if (e != cudaSuccess) return fail(errbuf, errcap, 2, "occupancy: %s", cudaGetErrorString(e));
     long long resident = (long long)sms * std::max(per_sm, 1) * (s->block / s->width);
     s->groups = (int)(s->cfg.wave_chains > 0 ? std::min<long long>(s->cfg.wave_chains, resident) : resident);

@@ -50,7 +50,8 @@ class Batch(ctypes.Structure):
                 ("out", ctypes.c_void_p), ("rec_off", ctypes.c_void_p), ("pkt_nsamp", ctypes.c_void_p),
                 ("pkt_rng", ctypes.c_void_p), ("res", ctypes.c_void_p), ("nchains", ctypes.c_int32),
                 ("width", ctypes.c_int32), ("schedule", ctypes.c_int32), ("max_groups", ctypes.c_int32),
-                ("order", ctypes.c_void_p), ("block", ctypes.c_int32), ("graph", ctypes.c_int32)]
+                ("order", ctypes.c_void_p), ("block", ctypes.c_int32), ("graph", ctypes.c_int32),
+                ("scalar", ctypes.c_int32)]
 
 
 _lib = None

@@ -111,6 +111,8 @@ typedef struct cuopus_batch {
     const uint32_t *order;
     int32_t block;
     int32_t graph;
+    int32_t scalar;      /* 1: only the first lane of each group decodes (lane-split loops run
+                            serially): the reference kernel's slot layout, for comparison */
 } cuopus_batch;
 
 int cuopus_decode_batch(const cuopus_batch *b, void *cuda_stream, float *kernel_ms, char *errbuf, size_t errcap);

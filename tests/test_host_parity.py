@@ -181,6 +181,24 @@ def test_host_decoder_matches_golden_libopus(hc, name):
         assert hashlib.sha256(pcm.astype("<i2").tobytes()).hexdigest() == g["pcm_sha256"], (name, i)
 
 
+@pytest.mark.parametrize("name", sorted(DECODE))
+def test_lane_loops_are_order_independent(name):
+    """The decoder built with every lane-split loop running backwards still
+    matches libopus: no iteration of such a loop reads what another writes,
+    which is what lets the GPU lanes run them in any order."""
+    rev = os.path.join(ROOT, "cuopus_b200", "lib", "libcuopus_hostcheck_rev.so")
+    if not os.path.exists(rev):
+        pytest.fail("libcuopus_hostcheck_rev.so must be built (python -m cuopus_b200.build)")
+    lib = ctypes.CDLL(rev)
+    ix = ogg_port.demux(_stream(name))
+    chains = [tuple(c) for c in INDEX[name]["chains_1_250"]]
+    got = host_decode(lib, ix["packets"], chains, ix["channels"])
+    for i, g in enumerate(DECODE[name]):
+        pcm, ns, rg, stop, samples = got[i]
+        assert [int(v) for v in rg] == g["rng"], (name, i)
+        assert hashlib.sha256(pcm.astype("<i2").tobytes()).hexdigest() == g["pcm_sha256"], (name, i)
+
+
 @pytest.mark.parametrize("seed", [11, 12, 13, 14])
 def test_host_decoder_matches_libopus_mixed(hc, seed):
     """Fresh seeded streams (SILK/hybrid/CELT, 2.5-60 ms, mono/stereo),
