@@ -12,7 +12,10 @@
 // tests hold the kernel to libopus on stereo streams.
 #define CUO_DECODE_KERNEL_TU 1
 #include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
 
+#include "../../include/cuopus.h"
 #include "kernels.cuh"
 
 namespace cuo {
@@ -32,4 +35,109 @@ cudaError_t decode_kernel_launch(const DecodeArgs &a, int blocks, int block, cud
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ allocation-free decode
+
+// Decoder slots of cuopus_decode_batch_noalloc: a fixed array in the
+// library's device image instead of a cudaMalloc'd workspace.  Every GPU that
+// loads the library holds it (CUOPUS_NOALLOC_MAX_SLOTS x sizeof(ChainSlot),
+// about 4.9 MiB) until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_slots[CUOPUS_NOALLOC_MAX_SLOTS * sizeof(ChainSlot)];
+
+// Device address of g_noalloc_slots per device, looked up once with that
+// device current.  In host code the array's name is only a host-side stand-in
+// for the symbol, never a device address, so the kernel gets this pointer.
+static void *g_noalloc_ptr[64];
+static bool g_noalloc_ready[64];
+
 } // namespace cuo
+
+static int noalloc_err(char *errbuf, size_t errcap, int rc, const char *msg, cudaError_t e)
+{
+    if (errbuf && errcap) {
+        if (e != cudaSuccess) snprintf(errbuf, errcap, "%s: %s", msg, cudaGetErrorString(e));
+        else snprintf(errbuf, errcap, "%s", msg);
+    }
+    return rc;
+}
+
+// The caller owns every table and output buffer (as in cuopus_decode_batch);
+// this entry point allocates nothing: decoder slots come from the static
+// array above, chains are dealt round-robin to at most
+// CUOPUS_NOALLOC_MAX_SLOTS resident groups, and no events, streams or graphs
+// are created.  Nothing in the slots needs clearing: a group initialises its
+// slot at the start of every chain and reads nothing it has not written.
+extern "C" int cuopus_decode_batch_noalloc(const cuopus_batch *b, void *cuda_stream, char *errbuf, size_t errcap)
+{
+    using namespace cuo;
+    if (errbuf && errcap) errbuf[0] = 0;
+    if (!b) return noalloc_err(errbuf, errcap, 3, "batch is NULL", cudaSuccess);
+    if (b->nchains <= 0) return 0;
+    int width = b->width > 0 ? b->width : 32;
+    if (width != 1 && width != 2 && width != 4 && width != 8 && width != 16 && width != 32)
+        return noalloc_err(errbuf, errcap, 3, "width is not a power of two <= 32", cudaSuccess);
+    int block = b->block > 0 ? b->block : 128;
+    if ((block != 32 && block != 64 && block != 96 && block != 128) || block % width)
+        return noalloc_err(errbuf, errcap, 3, "block must be 32, 64, 96 or 128 threads and a multiple of width",
+                           cudaSuccess);
+    if (!b->data || !b->off || !b->len || !b->first || !b->npkts || !b->channels || !b->trim || !b->keep ||
+        !b->res || (b->out && !b->out_off) || ((b->pkt_nsamp || b->pkt_rng) && !b->rec_off))
+        return noalloc_err(errbuf, errcap, 3, "batch has a NULL table", cudaSuccess);
+    if (b->max_groups > CUOPUS_NOALLOC_MAX_SLOTS) {
+        char m[128];
+        snprintf(m, sizeof m, "max_groups %d exceeds the %d static decoder slots", b->max_groups,
+                 CUOPUS_NOALLOC_MAX_SLOTS);
+        return noalloc_err(errbuf, errcap, 3, m, cudaSuccess);
+    }
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+        return noalloc_err(errbuf, errcap, 3, "refusing to decode during CUDA stream capture", cudaSuccess);
+    cudaGetLastError();
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return noalloc_err(errbuf, errcap, 2, "cudaGetDevice", e);
+    if (dev < 0 || dev >= 64) return noalloc_err(errbuf, errcap, 3, "device index out of range", cudaSuccess);
+    if (!g_noalloc_ready[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_slots);
+        if (e != cudaSuccess) return noalloc_err(errbuf, errcap, 2, "cudaGetSymbolAddress of the decoder slots", e);
+        g_noalloc_ptr[dev] = p;
+        g_noalloc_ready[dev] = true;
+    }
+    long long groups = b->nchains;
+    long long cap = b->max_groups > 0 ? b->max_groups : CUOPUS_NOALLOC_MAX_SLOTS;
+    if (groups > cap) groups = cap;
+    int gpb = block / width;
+    int blocks = (int)((groups + gpb - 1) / gpb);
+    if ((long long)blocks * gpb > CUOPUS_NOALLOC_MAX_SLOTS) blocks = CUOPUS_NOALLOC_MAX_SLOTS / gpb;
+    if (blocks < 1)
+        return noalloc_err(errbuf, errcap, 3, "block holds more groups than there are static slots", cudaSuccess);
+    DecodeArgs a;
+    memset(&a, 0, sizeof a);
+    a.data = b->data;
+    a.off = b->off;
+    a.len = b->len;
+    a.first = b->first;
+    a.npkts = b->npkts;
+    a.channels = b->channels;
+    a.trim = b->trim;
+    a.keep = b->keep;
+    a.out_off = b->out_off;
+    a.out = b->out;
+    a.order = nullptr;
+    a.rec_off = b->rec_off;
+    a.pkt_nsamp = b->pkt_nsamp;
+    a.pkt_rng = b->pkt_rng;
+    a.res = (ChainResult *)b->res;
+    a.slots = (ChainSlot *)g_noalloc_ptr[dev];
+    a.queue_head = nullptr;
+    a.nchains = b->nchains;
+    a.width = width;
+    a.use_queue = 0;
+    k_decode_chains<<<blocks, block, 0, st>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return noalloc_err(errbuf, errcap, 2, "decode launch", e);
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return noalloc_err(errbuf, errcap, 2, "decode", e);
+    return 0;
+}

@@ -117,6 +117,25 @@ typedef struct cuopus_batch {
 
 int cuopus_decode_batch(const cuopus_batch *b, void *cuda_stream, float *kernel_ms, char *errbuf, size_t errcap);
 
+/* Extension with no counterpart in the reference: cuopus_decode_batch for
+ * callers that cannot allocate device memory -- a process whose device memory
+ * is all handed to another framework's pool, or a latency-critical thread that
+ * must not call cudaMalloc / cudaFree (they can synchronise the whole device).
+ * The caller passes every table and output buffer, as for cuopus_decode_batch;
+ * the library allocates nothing: the decoder slots are a static device array
+ * of CUOPUS_NOALLOC_MAX_SLOTS slots (about 4.9 MiB) that every GPU loading the
+ * library holds until the process exits.  Chains are dealt round-robin to at
+ * most that many lane groups (schedule, order and graph of *b are ignored);
+ * max_groups above CUOPUS_NOALLOC_MAX_SLOTS is rejected with RC 3.  The first
+ * call on each device looks up the array's device address (with that device
+ * current), so make that first call before any stream capture; the call
+ * itself refuses to run during capture.  All calls share the one array:
+ * calls whose work overlaps on the GPU (other streams, other host threads)
+ * race on it and must be serialised by the caller.  Synchronises the stream
+ * before it returns. */
+#define CUOPUS_NOALLOC_MAX_SLOTS 64
+int cuopus_decode_batch_noalloc(const cuopus_batch *b, void *cuda_stream, char *errbuf, size_t errcap);
+
 /* Extension: autotuner of the decode launch.  Decodes the batch `reps` times
  * for every width in widths[0..nwidths) and block size in blocks[0..nblocks)
  * (the schedule, order and graph flag of *b are kept) and returns the pair
