@@ -1,6 +1,7 @@
 // Host-side Ogg-Opus demuxer and chain builder (see ogg_demux.h).
 #include "ogg_demux.h"
 
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -47,9 +48,46 @@ std::string fmt(const char *f, long long a = 0, long long b = 0, long long c = 0
     return buf;
 }
 
+// Ogg page CRC (RFC 3533): CRC-32, polynomial 0x04C11DB7, initial value 0,
+// no reflection, over the whole page with its checksum field taken as zero.
+uint32_t ogg_page_crc(const uint8_t *page, size_t len)
+{
+    static uint32_t table[256];
+    static bool init = false;
+    if (!init) {
+        for (uint32_t i = 0; i < 256; i++) {
+            uint32_t r = i << 24;
+            for (int k = 0; k < 8; k++) r = (r & 0x80000000u) ? (r << 1) ^ 0x04C11DB7u : r << 1;
+            table[i] = r;
+        }
+        init = true;
+    }
+    uint32_t crc = 0;
+    for (size_t i = 0; i < len; i++) {
+        uint8_t b = (i >= 22 && i < 26) ? 0 : page[i];
+        crc = (crc << 8) ^ table[((crc >> 24) ^ b) & 0xFF];
+    }
+    return crc;
+}
+
 } // namespace
 
+Options options_from_env()
+{
+    Options o;
+    const char *c = getenv("CUOPUS_OGG_CRC");
+    o.check_crc = c && atoi(c) > 0;
+    const char *g = getenv("CUOPUS_GRANULE");
+    o.granule_warn = g && strcmp(g, "warn") == 0;
+    return o;
+}
+
 bool demux(const uint8_t *data, size_t n, Demux &d, std::string &err)
+{
+    return demux(data, n, options_from_env(), d, err);
+}
+
+bool demux(const uint8_t *data, size_t n, const Options &opt, Demux &d, std::string &err)
 {
     d = Demux();
     if (!data || n == 0) { err = "empty stream"; return false; }
@@ -70,6 +108,14 @@ bool demux(const uint8_t *data, size_t n, Demux &d, std::string &err)
         uint64_t blen = 0;
         for (uint32_t i = 0; i < nseg; i++) blen += table[i];
         if (body + blen > n) break;
+        if (opt.check_crc) {
+            uint32_t stored = (uint32_t)data[idx + 22] | (uint32_t)data[idx + 23] << 8 |
+                              (uint32_t)data[idx + 24] << 16 | (uint32_t)data[idx + 25] << 24;
+            if (ogg_page_crc(data + idx, (size_t)(body + blen - idx)) != stored) {
+                err = fmt("page %lld: CRC mismatch", (long long)page_granule.size());
+                return false;
+            }
+        }
         uint32_t pg = (uint32_t)page_granule.size();
         page_granule.push_back(granule);
         uint64_t run_start = body;
@@ -174,6 +220,18 @@ bool demux(const uint8_t *data, size_t n, Demux &d, std::string &err)
     d.last_granule = last_granule;
     d.end_trim = d.toc_total - last_granule;
     d.play48 = last_granule - d.preskip;
+    if (opt.granule_warn && d.granule_match != d.granule_checked) {
+        // resync on the packets: their TOC durations are the timeline; the
+        // final granule still trims the end when it is a legal end trim
+        // (short of the TOC total by less than the last packet)
+        d.granule_mismatch = d.granule_checked - d.granule_match;
+        int64_t trim = d.toc_total - last_granule;
+        if (!(trim >= 0 && trim < last_dur)) trim = 0;
+        d.end_trim = trim;
+        d.last_granule = d.toc_total - trim;
+        d.play48 = d.last_granule - d.preskip;
+        d.granule_match = d.granule_checked;
+    }
     return true;
 }
 

@@ -39,16 +39,36 @@ struct Demux {
     int64_t end_trim = 0;
     uint32_t n_pages = 0;
     uint32_t granule_checked = 0, granule_match = 0;
+    uint32_t granule_mismatch = 0;    // pages resynchronised under the "warn" granule policy
     uint32_t n_packets() const { return (uint32_t)len.size(); }
 };
+
+// Demux options (extensions; the defaults are the reference's behaviour):
+//   check_crc     verify every page's CRC-32 (RFC 3533); a bad page fails the
+//                 stream (the reference's GPU path does not check, ogg_index.py
+//                 can: :103-111)
+//   granule_warn  a page granule that disagrees with the TOC durations does not
+//                 fail the stream: the packets' TOC durations are the timeline
+//                 and the final granule trims the end only when it is a legal
+//                 end trim (the reference fails such streams,
+//                 cuopus_demux.h:240-258)
+// options_from_env() reads them per call from CUOPUS_OGG_CRC=1 and
+// CUOPUS_GRANULE=warn.
+struct Options {
+    bool check_crc = false;
+    bool granule_warn = false;
+};
+Options options_from_env();
 
 struct Chains {
     std::vector<uint32_t> first, npkts, trim, keep;
     uint32_t size() const { return (uint32_t)first.size(); }
 };
 
-// Returns true on success; on failure `err` holds the reason.
+// Returns true on success; on failure `err` holds the reason.  The first form
+// takes its options from the environment.
 bool demux(const uint8_t *data, size_t n, Demux &d, std::string &err);
+bool demux(const uint8_t *data, size_t n, const Options &opt, Demux &d, std::string &err);
 bool build_chains(const Demux &d, double seconds, double preroll_ms, Chains &c, std::string &err);
 
 // Demux + the reference's acceptance checks (granule cross-check; mono only

@@ -122,6 +122,41 @@ def test_granule_mismatch_is_rejected(cn):
     assert e.value.rc == 1
 
 
+def test_granule_warn_policy_resyncs(cn, monkeypatch):
+    """CUOPUS_GRANULE=warn accepts the damaged granule and keeps the playable
+    length the packets and the (legal) final granule give."""
+    data = bytearray(_stream("mixed_mono_b"))
+    pages = []
+    p = data.find(b"OggS")
+    while p >= 0:
+        pages.append(p)
+        p = data.find(b"OggS", p + 4)
+    mid = pages[len(pages) // 2]
+    g = int.from_bytes(data[mid + 6:mid + 14], "little")
+    data[mid + 6:mid + 14] = (g + 480).to_bytes(8, "little")
+    monkeypatch.setenv("CUOPUS_GRANULE", "warn")
+    play, ch = cn.probe_pcm(bytes(data))
+    assert (play, ch) == (INDEX["mixed_mono_b"]["pcm_samples_48k"], 1)
+    ix = cn.index(bytes(data))
+    chains = [[int(a), int(b), int(c), int(d)] for a, b, c, d in zip(ix.first, ix.npkts, ix.trim, ix.keep)]
+    assert chains == INDEX["mixed_mono_b"]["chains_1_250"]
+
+
+def test_page_crc_check(cn, monkeypatch):
+    """CUOPUS_OGG_CRC=1 verifies every page checksum (RFC 3533)."""
+    data = _stream("plain_b")
+    assert cn.probe_pcm(data)[0] == INDEX["plain_b"]["pcm_samples_48k"]
+    monkeypatch.setenv("CUOPUS_OGG_CRC", "1")
+    assert cn.probe_pcm(data)[0] == INDEX["plain_b"]["pcm_samples_48k"]   # the corpus muxer writes valid CRCs
+    bad = bytearray(data)
+    bad[len(bad) // 2] ^= 0x40                                             # one payload bit
+    with pytest.raises(cn.CuopusError) as e:
+        cn.probe_pcm(bytes(bad))
+    assert e.value.rc == 1 and "CRC" in str(e.value)
+    monkeypatch.delenv("CUOPUS_OGG_CRC")
+    cn.probe_pcm(bytes(bad))                                               # not checked by default
+
+
 # ------------------------------------------------------------------ host same-source decoder
 
 def test_range_decoder_gate_schedules(hc):
