@@ -449,7 +449,16 @@ DNI void deemphasis(Lanes L, int32_t *in0, int32_t *in1, int16_t *pcm, int N, in
                     int accum)
 {
     const int16_t coef0 = T_CELT_PREEMPH0;
-    for (int c = 0; c < C; c++) {
+    // The channels are independent recursions: with two or more lanes, lane c
+    // runs channel c, so a stereo frame's two recursions execute side by side
+    // in the same instructions; a single lane runs them one after the other.
+    lsync(L);
+    int c0 = 0, c1 = C;
+    if (L.n > 1) {
+        c0 = L.id;
+        c1 = L.id < C ? L.id + 1 : L.id;
+    }
+    for (int c = c0; c < c1; c++) {
         const int32_t *x = c == 0 ? in0 : in1;
         int16_t *y = pcm + c;
         int32_t m = mem[c];

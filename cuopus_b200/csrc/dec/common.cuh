@@ -66,6 +66,18 @@ DFN void lsync(const Lanes &L)
 #define LFOR(L, i, start, end) for (int i = (start) + (L).id; i < (end); i += (L).n)
 #endif
 
+// Sum of v over the lanes of the group with wrap-around 32-bit adds (so the
+// order of the terms does not change the result); every lane gets the total.
+DFN int32_t lsum(const Lanes &L, int32_t v)
+{
+#ifdef __CUDA_ARCH__
+    for (int off = L.n >> 1; off > 0; off >>= 1) v = (int32_t)((uint32_t)v + (uint32_t)__shfl_xor_sync(L.mask, v, off));
+#else
+    (void)L;
+#endif
+    return v;
+}
+
 // buf[i] = buf[i + shift] for i = 0 .. n-1 (the forward in-place copy that
 // drops the oldest `shift` samples of a history buffer), split across the
 // lanes.  Positions go in blocks of `shift`: block k reads only block k+1,

@@ -125,16 +125,18 @@ enum { RS_TAPS = 49, RS_PAD = 24, RS_OUT_PER_THREAD = 4, RS_THREADS = 256,
 
 __constant__ float c_rs_taps[RS_TAPS];
 
-// out[i] for i in [0, n_out): taps over in[3 i - 24 + t], in valid on [0, avail)
+// out[i * chans] for i in [0, n_out): taps over in[(3 i - 24 + t) * chans], the
+// input valid for sample indices [0, avail); chans > 1 resamples one channel of
+// an interleaved stream into one channel of an interleaved output.
 __global__ void __launch_bounds__(RS_THREADS) k_resample48to16(const int16_t *__restrict__ in, long long avail,
-                                                               long long n_out, float *__restrict__ out)
+                                                               long long n_out, float *__restrict__ out, int chans)
 {
     __shared__ float xs[RS_TILE_IN];
     const long long o0 = (long long)blockIdx.x * RS_TILE_OUT;
     const long long base = 3 * o0 - RS_PAD;
     for (int i = threadIdx.x; i < RS_TILE_IN; i += RS_THREADS) {
         long long g = base + i;
-        xs[i] = (g >= 0 && g < avail) ? (float)in[g] * (1.0f / 32768.0f) : 0.0f;
+        xs[i] = (g >= 0 && g < avail) ? (float)in[g * chans] * (1.0f / 32768.0f) : 0.0f;
     }
     __syncthreads();
     const int j0 = threadIdx.x * RS_OUT_PER_THREAD;
@@ -148,12 +150,12 @@ __global__ void __launch_bounds__(RS_THREADS) k_resample48to16(const int16_t *__
         acc[k] = a;
     }
     long long i0 = o0 + j0;
-    if (i0 + RS_OUT_PER_THREAD <= n_out && ((((uintptr_t)(out + i0)) & 15) == 0)) {
+    if (chans == 1 && i0 + RS_OUT_PER_THREAD <= n_out && ((((uintptr_t)(out + i0)) & 15) == 0)) {
         *reinterpret_cast<float4 *>(out + i0) = make_float4(acc[0], acc[1], acc[2], acc[3]);
     } else {
 #pragma unroll
         for (int k = 0; k < RS_OUT_PER_THREAD; k++)
-            if (i0 + k < n_out) out[i0 + k] = acc[k];
+            if (i0 + k < n_out) out[(i0 + k) * chans] = acc[k];
     }
 }
 #endif

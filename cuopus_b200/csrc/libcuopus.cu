@@ -534,20 +534,25 @@ int64_t out16_of(int64_t play48)
     return v < 0 ? 0 : v;
 }
 
-int resample(const int16_t *in, int64_t avail, int64_t n_out, float *out, cudaStream_t st, Err &err)
+int resample(const int16_t *in, int64_t avail, int64_t n_out, float *out, cudaStream_t st, Err &err, int chans = 1)
 {
     if (n_out <= 0) return RC_OK;
     int rc = ensure_taps(st, err);
     if (rc) return rc;
     long long blocks = (n_out + cuo::RS_TILE_OUT - 1) / cuo::RS_TILE_OUT;
     if (blocks > 0x7fffffffLL) return err.set(RC_ARG, "resample length too large");
-    cuo::k_resample48to16<<<(unsigned)blocks, cuo::RS_THREADS, 0, st>>>(in, avail, n_out, out);
+    cuo::k_resample48to16<<<(unsigned)blocks, cuo::RS_THREADS, 0, st>>>(in, avail, n_out, out, chans);
     CK(cudaGetLastError());
     return RC_OK;
 }
 
+// f16k decode of N files.  The reference entry points are mono only
+// (allow_stereo false); with allow_stereo each channel of a stereo file is
+// resampled on its own and the output interleaves them (out_caps then count
+// floats over all channels).
 int f16k_impl(const uint8_t *const *oggs, const size_t *ns, int nfiles, float *const *out_devs,
-              const size_t *out_caps, int64_t *out_lens, cudaStream_t st, bool enforce_max_batch, Err &err)
+              const size_t *out_caps, int64_t *out_lens, cudaStream_t st, bool enforce_max_batch, Err &err,
+              bool allow_stereo = false, int32_t *out_channels = nullptr)
 {
     G.last_ovf = 0;
     if (out_lens) for (int f = 0; f < nfiles; f++) out_lens[f] = 0;
@@ -557,7 +562,7 @@ int f16k_impl(const uint8_t *const *oggs, const size_t *ns, int nfiles, float *c
     Plan P;
     G.last = cuopus_stats{};
     double t0 = now_ms();
-    if ((rc = plan_files(oggs, ns, nfiles, true, P, err))) return rc;
+    if ((rc = plan_files(oggs, ns, nfiles, !allow_stereo, P, err))) return rc;
     G.last.demux_ms = now_ms() - t0;
     if (P.first.empty()) return err.set(RC_SOFT, "no chains");
     if (enforce_max_batch) {
@@ -569,9 +574,10 @@ int f16k_impl(const uint8_t *const *oggs, const size_t *ns, int nfiles, float *c
     std::vector<int64_t> n16(nfiles);
     for (int f = 0; f < nfiles; f++) {
         n16[f] = out16_of((int64_t)P.file_keep[f]);   // sum(keep) == playable samples
-        if (!out_caps || (uint64_t)n16[f] > out_caps[f])
-            return err.set(RC_ARG, "file %d: output capacity %zu < required %lld", f, out_caps ? out_caps[f] : 0,
-                           (long long)n16[f]);
+        uint64_t need = (uint64_t)n16[f] * (uint64_t)P.file_chans[f];
+        if (!out_caps || need > out_caps[f])
+            return err.set(RC_ARG, "file %d: output capacity %zu < required %llu", f, out_caps ? out_caps[f] : 0,
+                           (unsigned long long)need);
         if (n16[f] > 0 && (!out_devs || !out_devs[f])) return err.set(RC_ARG, "file %d: out_dev is NULL", f);
     }
     int64_t total16 = 0;
@@ -580,13 +586,17 @@ int f16k_impl(const uint8_t *const *oggs, const size_t *ns, int nfiles, float *c
     if ((rc = run_plan(P, st, err))) return rc;
     CK(cudaEventRecord(G.evr0, st));
     for (int f = 0; f < nfiles; f++) {
-        const int16_t *in = (const int16_t *)G.pcm.p + P.file_out0[f];
-        if ((rc = resample(in, (int64_t)P.file_keep[f], n16[f], out_devs[f], st, err))) return rc;
+        int ch = P.file_chans[f];
+        for (int c = 0; c < ch; c++) {
+            const int16_t *in = (const int16_t *)G.pcm.p + P.file_out0[f] + c;
+            if ((rc = resample(in, (int64_t)P.file_keep[f], n16[f], out_devs[f] + c, st, err, ch))) return rc;
+        }
     }
     CK(cudaEventRecord(G.evr1, st));
     if ((rc = validate(P, st, err))) return rc;
     record_stats(P, true);
     if (out_lens) for (int f = 0; f < nfiles; f++) out_lens[f] = n16[f];
+    if (out_channels) for (int f = 0; f < nfiles; f++) out_channels[f] = P.file_chans[f];
     return RC_OK;
 }
 
@@ -727,6 +737,16 @@ extern "C" int cuopus_decode_f16k_multi(const uint8_t *const *oggs, const size_t
     std::lock_guard<std::mutex> lk(g_mu);
     Err err(errbuf, errcap);
     return f16k_impl(oggs, ns, nfiles, out_devs, out_caps, out_lens, (cudaStream_t)cuda_stream, nfiles > 1, err);
+}
+
+extern "C" int cuopus_decode_f16k_channels(const uint8_t *const *oggs, const size_t *ns, int nfiles,
+                                           float *const *out_devs, const size_t *out_caps, int64_t *out_lens,
+                                           int32_t *out_channels, void *cuda_stream, char *errbuf, size_t errcap)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    Err err(errbuf, errcap);
+    return f16k_impl(oggs, ns, nfiles, out_devs, out_caps, out_lens, (cudaStream_t)cuda_stream, false, err, true,
+                     out_channels);
 }
 
 extern "C" int cuopus_decode_i16_multi(const uint8_t *const *oggs, const size_t *ns, int nfiles,

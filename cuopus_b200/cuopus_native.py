@@ -233,6 +233,40 @@ def decode_ogg_multi(items):
     return outs
 
 
+def decode_ogg_to_f16k_channels(items):
+    """Extension: float32 16 kHz output for mono and stereo files (stereo
+    channels resampled separately, interleaved).  Returns a list of
+    (tensor[float32, samples*channels], channels)."""
+    import torch
+    lib = _load()
+    if not getattr(lib, "_f16kc_bound", False):
+        lib.cuopus_decode_f16k_channels.restype = ctypes.c_int
+        lib.cuopus_decode_f16k_channels.argtypes = [
+            ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_size_t), ctypes.c_int,
+            ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int64),
+            ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+        lib._f16kc_bound = True
+    blobs = [_as_bytes(x) for x in items]
+    n = len(blobs)
+    if n == 0:
+        return []
+    caps = []
+    for b in blobs:
+        play, ch = probe_pcm(b)
+        caps.append(max(0, (play - 48) // 3) * ch)
+    outs = [torch.empty(max(c, 1), dtype=torch.float32, device="cuda") for c in caps]
+    stream = torch.cuda.current_stream().cuda_stream
+    ba = (ctypes.c_char_p * n)(*blobs)
+    la = (ctypes.c_size_t * n)(*[len(b) for b in blobs])
+    oa = (ctypes.c_void_p * n)(*[o.data_ptr() for o in outs])
+    ca = (ctypes.c_size_t * n)(*caps)
+    ol = (ctypes.c_int64 * n)()
+    oc = (ctypes.c_int32 * n)()
+    err = ctypes.create_string_buffer(_ERRCAP)
+    _check(lib.cuopus_decode_f16k_channels(ba, la, n, oa, ca, ol, oc, ctypes.c_void_p(stream), err, _ERRCAP), err)
+    return [(outs[i][:ol[i] * oc[i]], oc[i]) for i in range(n)]
+
+
 def decode_ogg_to_int16(items, capacities=None):
     """Extension: decode files to 48 kHz interleaved int16 playable PCM (mono or
     stereo).  Returns a list of (tensor[int16, samples*channels], channels)."""

@@ -67,6 +67,16 @@ void cuopus_release_workspaces(void);
 
 /* ------------------------------------------------------------------ extensions */
 
+/* Extension (no counterpart in the reference, whose f16k paths reject stereo):
+ * cuopus_decode_f16k_multi for mono and stereo files.  Each channel of a
+ * stereo file is resampled on its own with the same filter and the float32
+ * 16 kHz output interleaves the channels; out_caps count floats over all
+ * channels, out_lens receive samples per channel, out_channels (may be NULL)
+ * the channel count.  Mono output equals cuopus_decode_f16k_multi's. */
+int cuopus_decode_f16k_channels(const uint8_t *const *oggs, const size_t *ns, int nfiles, float *const *out_devs,
+                                const size_t *out_caps, int64_t *out_lens, int32_t *out_channels, void *cuda_stream,
+                                char *errbuf, size_t errcap);
+
 /* Extension (the reference CLI's int16 "DECODE" output, for mono and stereo):
  * decode N files to 48 kHz interleaved int16 playable PCM.  out_caps are in
  * int16 elements; out_lens receive samples per channel; out_channels (may be

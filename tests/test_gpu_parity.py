@@ -109,6 +109,25 @@ def test_f16k_multi_equals_single(cuda):
         assert a.shape == b.shape and np.array_equal(a, b)
 
 
+def test_f16k_channels_stereo_and_mono(cuda):
+    """Stereo f16k: each channel resampled by the same filter, interleaved;
+    max abs diff 0 against the resampler restatement per channel."""
+    from cuopus_b200 import cuopus_native as cn
+    streams = _streams("mixed", 4, 2.5, 8400)
+    outs = cn.decode_ogg_to_f16k_channels(streams)
+    for d, (t, ch) in zip(streams, outs):
+        pcm, wch, _ = pipeline.i16(d)
+        assert ch == wch
+        play = pcm.size // ch
+        n16 = max(0, (play - 48) // 3)
+        want = np.stack([pipeline.resample(np.ascontiguousarray(pcm[c::ch]), n16) for c in range(ch)], 1).reshape(-1)
+        got = t.cpu().numpy()
+        assert got.shape == want.shape
+        assert np.max(np.abs(got - want), initial=0.0) == 0.0
+        if ch == 1:
+            assert np.array_equal(got, cn.decode_ogg_to_cuda_tensor(d).cpu().numpy())
+
+
 def test_i16_stereo_and_mono(cuda):
     from cuopus_b200 import cuopus_native as cn
     streams = _streams("mixed", 4, 3.0, 8300)
