@@ -285,7 +285,7 @@ def schedule_batch(cn, db, stream, args):
                      "lane_split": {"ms_per_step": plain_ms, "value": db.audio_s / (plain_ms / 1e3),
                                     "schedule": "plain one-launch, one warp per chain, 32 lanes, index order"}}
     res = db.results()
-    cycles = res[:, 3].astype(np.float64)
+    cycles = res[:, 3].astype(np.float64)     # decode time per chain (us), the cost model's target
     # learned order (the packet-count order is the fallback)
     order = costmodel.packet_order(db.cap_pkts, db.chans)
     info["order"] = "packets x channels"
@@ -395,6 +395,46 @@ def serve_bench(args, files, dev):
 
 # ------------------------------------------------------------------ main
 
+def phases_report(args):
+    """Split of the decoder's time between its stages, from the stage timers of
+    the diagnostic build: one decode of the workload in the lane-split form
+    (the --width / --block given, packet-count order, queue schedule) and one
+    in the one-lane reference layout.  Prints one JSON line (not a bench line:
+    the timers cost time of their own)."""
+    import torch
+    from cuopus_b200 import cuopus_native as cn
+    os.environ["CUOPUS_LIB"] = cn.phases_lib_path()     # before the library is first loaded
+    from cuopus_b200 import costmodel
+    torch.cuda.set_device(0)
+    files, seg = load_inputs(args.workload, args.count)
+    cn.warmup()
+    db = DeviceBatch(files, seg, "cuda:0")
+    stream = torch.cuda.current_stream()
+    order = costmodel.packet_order(db.cap_pkts, db.chans)
+    # DeviceBatch.batch() keeps the order array of the latest batch alive only,
+    # so each batch is made right before its use
+    forms = {"lane_split": lambda: db.batch(args.width, 1, order, args.block, 0),
+             "one_lane": lambda: db.batch(32, 2, None, 128, 0, scalar=1)}
+    out = {"report": "decoder stage cycles", "workload": args.workload, "chains": db.n,
+           "audio_s": round(db.audio_s, 1), "width": args.width, "block": args.block}
+    for name, make in forms.items():
+        b = make()
+        cn.decode_batch(b, stream.cuda_stream)     # warm
+        torch.cuda.synchronize()
+        cn.phase_reset()
+        ms = cn.decode_batch(b, stream.cuda_stream)
+        torch.cuda.synchronize()
+        ph = cn.phase_cycles()
+        chain_us = float(db.results()[:, 3].astype(np.float64).sum())
+        tot = float(ph["packet"]) or 1.0
+        out[name] = {"kernel_ms_with_timers": round(ms, 2), "chain_seconds": round(chain_us / 1e6, 2),
+                     "cycles_per_audio_s": {k: round(v / db.audio_s) for k, v in ph.items()},
+                     "share_of_packet": {k: round(v / tot, 4) for k, v in ph.items() if k != "packet"}}
+        log(name, json.dumps(out[name]["share_of_packet"]))
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -412,6 +452,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--rate", type=float, default=100.0, help="serve: Poisson arrivals per second")
     ap.add_argument("--budget-gb", type=int, default=40, help="serve: admission budget")
+    ap.add_argument("--phases", action="store_true",
+                    help="diagnostics, not a bench line: per-stage decoder cycles from libcuopus_phases.so")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -441,6 +483,9 @@ def main():
                 "e2e": {"value": v, "unit": "audio-s/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return 0
+
+    if args.phases:
+        return phases_report(args)
 
     import torch
     if world > 1:
@@ -495,12 +540,10 @@ def main():
     barrier()
     value = world * db.audio_s / (step_ms / 1e3)
     kern_ms = statistics.mean(kern)
-    # the makespan floor: the most expensive single chain, from the cycles the
-    # decoder records per chain (at the sampled SM clock)
-    cyc = db.results()[:, 3].astype(np.float64)
-    clk_s = clk.summary() or {}
-    mhz = clk_s.get("sm_mhz") or 1965.0
-    tail = {"longest_chain_ms": float(cyc.max() / (mhz * 1e3)), "chain_seconds_total": float(cyc.sum() / (mhz * 1e6)),
+    # the makespan floor: the most expensive single chain, from the decode time
+    # the decoder records per chain
+    us = db.results()[:, 3].astype(np.float64)
+    tail = {"longest_chain_ms": float(us.max() / 1e3), "chain_seconds_total": float(us.sum() / 1e6),
             "kernel_ms": kern_ms}
     alg_bytes = db.pkt_bytes + db.pcm_bytes
     pk = peaks()

@@ -2,6 +2,8 @@
 
   cuopus_b200/lib/libcuopus.so            the product: CUDA kernels for sm_100a
                                           plus the C ABI of include/cuopus.h
+  cuopus_b200/lib/libcuopus_phases.so     the same with the decoder's stage timers
+                                          (diagnostics: python -m cuopus_b200.phase_profile)
   cuopus_b200/lib/libcuopus_hostcheck.so  the same decoder sources compiled for
                                           the host (g++), used only by tests
   cuopus_b200/bin/cuopus_decode           the command-line tool / daemon
@@ -24,6 +26,7 @@ NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 LIBCUOPUS = os.path.join(LIB, "libcuopus.so")
+LIBPHASES = os.path.join(LIB, "libcuopus_phases.so")
 HOSTCHECK = os.path.join(LIB, "libcuopus_hostcheck.so")
 HOSTCHECK_REV = os.path.join(LIB, "libcuopus_hostcheck_rev.so")
 CLI = os.path.join(BIN, "cuopus_decode")
@@ -72,10 +75,15 @@ def build_libcuopus(force=False):
     _run(common + ["-c", os.path.join(CSRC, "server.cu"), "-o", os.path.join(obj, "server.o")])
     _run(common + ["-c", os.path.join(CSRC, "ogg_demux.cpp"), "-o", os.path.join(obj, "ogg_demux.o")])
     tmp = LIBCUOPUS + ".tmp"
-    _run([NVCC, *ARCH, "-shared", "-o", tmp] +
-         [os.path.join(obj, o) for o in ("decode_kernel.o", "libcuopus.o", "costmodel.o", "server.o",
-                                         "ogg_demux.o")])
+    rest = [os.path.join(obj, o) for o in ("libcuopus.o", "costmodel.o", "server.o", "ogg_demux.o")]
+    _run([NVCC, *ARCH, "-shared", "-o", tmp, os.path.join(obj, "decode_kernel.o")] + rest)
     os.replace(tmp, LIBCUOPUS)
+    # diagnostic build: the same library with the decoder's stage timers on
+    _run(common + ["-Xcicc", "-O1", "-Xptxas", "-O1", "-DCUO_PHASE_TIMERS", "-c",
+                   os.path.join(CSRC, "decode_kernel.cu"), "-o", os.path.join(obj, "decode_kernel_phases.o")])
+    tmp = LIBPHASES + ".tmp"
+    _run([NVCC, *ARCH, "-shared", "-o", tmp, os.path.join(obj, "decode_kernel_phases.o")] + rest)
+    os.replace(tmp, LIBPHASES)
     return LIBCUOPUS
 
 

@@ -4,7 +4,7 @@ kernels in csrc/costmodel.cu, reached through the C ABI).
 A chain's decode time is predicted from 16 features of its packets' TOC
 bytes (mode, frame sizes, bandwidth, channels, sizes) by an FP32 MLP
 16 -> 64 -> 64 -> 1 with ReLU, trained on the GPU on log cycle counts that the
-decoder itself records per chain (res[c].cycles).  The queue schedule then
+decoder itself records per chain (res[c].time_us).  The queue schedule then
 visits chains longest first by prediction.  The fallback, and the baseline the
 model is judged against, is the packet-count order (packets x channels).
 
@@ -66,7 +66,7 @@ def packet_order(npkts, channels):
 
 
 class CostModel:
-    """FP32 MLP over chain features; targets are standardised log cycles."""
+    """FP32 MLP over chain features; targets are standardised log decode times."""
 
     def __init__(self, seed=0):
         import torch
@@ -86,11 +86,11 @@ class CostModel:
               ctypes.c_void_p(loss.data_ptr()), _stream())
         return float(loss.item()), g
 
-    def fit(self, X, cycles, steps=2000, lr=3e-3):
-        """Train on device features X [n, 16] and measured cycles (host or
+    def fit(self, X, cost, steps=2000, lr=3e-3):
+        """Train on device features X [n, 16] and measured decode times (host or
         device, > 0).  Returns the per-step losses."""
         import torch
-        y = np.log(np.maximum(np.asarray(torch.as_tensor(cycles).cpu().numpy(), np.float64), 1.0))
+        y = np.log(np.maximum(np.asarray(torch.as_tensor(cost).cpu().numpy(), np.float64), 1.0))
         self.mu, self.sigma = float(y.mean()), float(y.std() or 1.0)
         T = torch.from_numpy(((y - self.mu) / self.sigma).astype(np.float32)).cuda()
         X = X.contiguous().float()
@@ -101,7 +101,7 @@ class CostModel:
         return losses[:steps]
 
     def predict_raw(self, X):
-        """Network outputs (standardised log cycles) as a device tensor."""
+        """Network outputs (standardised log decode times) as a device tensor."""
         import torch
         X = X.contiguous().float()
         y = torch.empty(max(int(X.shape[0]), 1), dtype=torch.float32, device="cuda")
@@ -110,12 +110,12 @@ class CostModel:
         return y[:X.shape[0]]
 
     def predict(self, X):
-        """Predicted cycles per chain (host float64)."""
+        """Predicted decode time per chain (host float64, the unit of the targets)."""
         y = self.predict_raw(X).cpu().numpy().astype(np.float64)
         return np.exp(y * self.sigma + self.mu)
 
     def order(self, X):
-        """Longest-first visiting order by predicted cycles (stable)."""
+        """Longest-first visiting order by predicted decode time (stable)."""
         return np.argsort(-self.predict(X), kind="stable")
 
     def state(self):

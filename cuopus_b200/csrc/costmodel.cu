@@ -1,6 +1,6 @@
 // Learned cost model of the decode scheduler: per-chain features from the
 // packets' TOC bytes, and an FP32 multilayer perceptron (16 -> 64 -> 64 -> 1,
-// ReLU) that predicts log decode cycles of a chain, trained and evaluated
+// ReLU) that predicts the log decode time of a chain, trained and evaluated
 // with the kernels below.  The queue schedule of the decoder visits chains in
 // decreasing predicted cost (longest first); the packet-count order is the
 // fallback.  None of this changes a decoded sample: it only orders the work.

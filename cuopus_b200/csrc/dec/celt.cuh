@@ -1137,105 +1137,177 @@ DNI unsigned quant_band_n1(BandCtx *ctx, int16_t *X, int16_t *Y, int16_t *lowban
     return 1;
 }
 
-// celt/bands.c quant_partition; LMP1 = LM + 1 bounds the split depth
-template <int LMP1>
-DNI unsigned quant_partition(BandCtx *ctx, int16_t *X, int N, int b, int B, int16_t *lowband, int16_t gain,
-                             int fill)
+// celt/bands.c quant_partition, leaf: pulses for the band piece (PVQ) or,
+// with none, folding / noise fill.
+DNI unsigned quant_partition_leaf(BandCtx *ctx, int16_t *X, int N, int b, int B, int16_t *lowband, int LM,
+                                  int16_t gain, int fill)
 {
-    const int LM = LMP1 - 1;
-    int i = ctx->i;
-    const uint8_t *cache = T_celt_cache_bits + T_celt_cache_index[(LM + 1) * CELT_NB + i];
+    const int i = ctx->i;
     unsigned cm = 0;
-    if constexpr (LMP1 > 0) {
-    if (b > cache[cache[0]] + 12 && N > 2) {
-        int B0 = B;
-        SplitCtx sctx;
-        int16_t *next_lowband2 = 0;
-        N >>= 1;
-        int16_t *Y = X + N;
-        if (B == 1) fill = (fill & 1) | (fill << 1);
-        B = (B + 1) >> 1;
-        compute_theta(ctx, &sctx, N, &b, B, B0, LM - 1, 0, &fill);
-        int16_t mid = (int16_t)sctx.imid, side = (int16_t)sctx.iside;
-        int delta = sctx.delta, itheta = sctx.itheta;
-        if (B0 > 1 && (itheta & 0x3fff)) {
-            if (itheta > 8192) delta -= delta >> (4 - (LM - 1));
-            else delta = imin(0, delta + (N << 3 >> (5 - (LM - 1))));
-        }
-        int mbits = imax(0, imin(b, (b - delta) / 2));
-        int sbits = b - mbits;
-        ctx->remaining_bits -= sctx.qalloc;
-        if (lowband) next_lowband2 = lowband + N;
-        int32_t rebalance = ctx->remaining_bits;
-        if (mbits >= sbits) {
-            cm = quant_partition<(LMP1 > 0 ? LMP1 - 1 : 0)>(ctx, X, N, mbits, B, lowband,
-                                                            (int16_t)c_mul16_p15(gain, mid), fill);
-            rebalance = mbits - (rebalance - ctx->remaining_bits);
-            if (rebalance > 3 << 3 && itheta != 0) sbits += rebalance - (3 << 3);
-            cm |= quant_partition<(LMP1 > 0 ? LMP1 - 1 : 0)>(ctx, Y, N, sbits, B, next_lowband2,
-                                                             (int16_t)c_mul16_p15(gain, side), fill >> B)
-                  << (B0 >> 1);
-        } else {
-            cm = quant_partition<(LMP1 > 0 ? LMP1 - 1 : 0)>(ctx, Y, N, sbits, B, next_lowband2,
-                                                            (int16_t)c_mul16_p15(gain, side), fill >> B)
-                 << (B0 >> 1);
-            rebalance = sbits - (rebalance - ctx->remaining_bits);
-            if (rebalance > 3 << 3 && itheta != 16384) mbits += rebalance - (3 << 3);
-            cm |= quant_partition<(LMP1 > 0 ? LMP1 - 1 : 0)>(ctx, X, N, mbits, B, lowband,
-                                                             (int16_t)c_mul16_p15(gain, mid), fill);
-        }
-        return cm;
-    }
-    }
-    {
-        int q = bits2pulses(i, LM, b);
-        int curr_bits = pulses2bits(i, LM, q);
+    int q = bits2pulses(i, LM, b);
+    int curr_bits = pulses2bits(i, LM, q);
+    ctx->remaining_bits -= curr_bits;
+    while (ctx->remaining_bits < 0 && q > 0) {
+        ctx->remaining_bits += curr_bits;
+        q--;
+        curr_bits = pulses2bits(i, LM, q);
         ctx->remaining_bits -= curr_bits;
-        while (ctx->remaining_bits < 0 && q > 0) {
-            ctx->remaining_bits += curr_bits;
-            q--;
-            curr_bits = pulses2bits(i, LM, q);
-            ctx->remaining_bits -= curr_bits;
-        }
-        if (q != 0) {
-            int K = get_pulses(q);
-            cm = alg_unquant(X, N, K, ctx->spread, B, ctx->ec, gain, ctx->w->iy);
+    }
+    if (q != 0) {
+        int K = get_pulses(q);
+        cm = alg_unquant(X, N, K, ctx->spread, B, ctx->ec, gain, ctx->w->iy);
+    } else {
+        unsigned cm_mask = (unsigned)(1UL << B) - 1;
+        fill &= cm_mask;
+        if (!fill) {
+            for (int j = 0; j < N; j++) X[j] = 0;
         } else {
-            unsigned cm_mask = (unsigned)(1UL << B) - 1;
-            fill &= cm_mask;
-            if (!fill) {
-                for (int j = 0; j < N; j++) X[j] = 0;
-            } else {
-                if (lowband == 0) {
-                    for (int j = 0; j < N; j++) {
-                        ctx->seed = c_lcg_rand(ctx->seed);
-                        X[j] = (int16_t)((int32_t)ctx->seed >> 20);
-                    }
-                    cm = cm_mask;
-                } else {
-                    for (int j = 0; j < N; j++) {
-                        ctx->seed = c_lcg_rand(ctx->seed);
-                        int16_t tmp = (ctx->seed & 0x8000) ? 4 : -4;   // QCONST16(1.0f/256, 10)
-                        X[j] = (int16_t)(lowband[j] + tmp);
-                    }
-                    cm = fill;
+            if (lowband == 0) {
+                for (int j = 0; j < N; j++) {
+                    ctx->seed = c_lcg_rand(ctx->seed);
+                    X[j] = (int16_t)((int32_t)ctx->seed >> 20);
                 }
-                renormalise_vector(X, N, gain);
+                cm = cm_mask;
+            } else {
+                for (int j = 0; j < N; j++) {
+                    ctx->seed = c_lcg_rand(ctx->seed);
+                    int16_t tmp = (ctx->seed & 0x8000) ? 4 : -4;   // QCONST16(1.0f/256, 10)
+                    X[j] = (int16_t)(lowband[j] + tmp);
+                }
+                cm = fill;
             }
+            renormalise_vector(X, N, gain);
         }
     }
     return cm;
 }
 
-DFN unsigned quant_partition_lm(BandCtx *ctx, int16_t *X, int N, int b, int B, int16_t *lowband, int LM,
-                                int16_t gain, int fill)
+// celt/bands.c quant_partition.  libopus recurses into the two halves of a
+// split band; here one loop walks an explicit stack of frames instead, so a
+// single copy of the code serves every depth (the split depth is bounded by
+// LM + 1 <= 4, five frames).  A frame resumes after each half: stage 1 / 2
+// when the mid half went first, 3 / 4 when the side half did; the bit
+// rebalancing between the halves and the collapse-mask combination happen at
+// those points, in libopus's order.
+struct QPFrame {
+    int16_t *X, *Y, *lowband, *next_lowband2;
+    int N, b, B, B0, LM, fill, mbits, sbits, itheta, stage;
+    int32_t rebalance;
+    int16_t gain, mid, side;
+    unsigned cm;
+};
+
+DNI unsigned quant_partition(BandCtx *ctx, int16_t *X, int N, int b, int B, int16_t *lowband, int LM,
+                             int16_t gain, int fill)
 {
-    switch (LM) {
-    case 0: return quant_partition<1>(ctx, X, N, b, B, lowband, gain, fill);
-    case 1: return quant_partition<2>(ctx, X, N, b, B, lowband, gain, fill);
-    case 2: return quant_partition<3>(ctx, X, N, b, B, lowband, gain, fill);
-    default: return quant_partition<4>(ctx, X, N, b, B, lowband, gain, fill);
+    QPFrame st[5];
+    int sp = 0;
+    st[0].X = X;
+    st[0].N = N;
+    st[0].b = b;
+    st[0].B = B;
+    st[0].lowband = lowband;
+    st[0].LM = LM;
+    st[0].gain = gain;
+    st[0].fill = fill;
+    st[0].stage = 0;
+    unsigned ret = 0;
+    const int i = ctx->i;
+    while (sp >= 0) {
+        QPFrame *f = &st[sp];
+        QPFrame *c = &st[sp + 1 < 5 ? sp + 1 : 4];
+        if (f->stage == 0) {
+            const uint8_t *cache = T_celt_cache_bits + T_celt_cache_index[(f->LM + 1) * CELT_NB + i];
+            if (f->LM != -1 && f->b > cache[cache[0]] + 12 && f->N > 2 && sp < 4) {
+                SplitCtx sctx;
+                int B0 = f->B;
+                int N2 = f->N >> 1;
+                int fill2 = f->fill;
+                if (f->B == 1) fill2 = (fill2 & 1) | (fill2 << 1);
+                int B2 = (f->B + 1) >> 1;
+                int LM2 = f->LM - 1;
+                int b2 = f->b;
+                compute_theta(ctx, &sctx, N2, &b2, B2, B0, LM2, 0, &fill2);
+                int delta = sctx.delta, itheta = sctx.itheta;
+                if (B0 > 1 && (itheta & 0x3fff)) {
+                    if (itheta > 8192) delta -= delta >> (4 - LM2);
+                    else delta = imin(0, delta + (N2 << 3 >> (5 - LM2)));
+                }
+                int mbits = imax(0, imin(b2, (b2 - delta) / 2));
+                int sbits = b2 - mbits;
+                ctx->remaining_bits -= sctx.qalloc;
+                f->Y = f->X + N2;
+                f->N = N2;
+                f->B = B2;
+                f->B0 = B0;
+                f->LM = LM2;
+                f->fill = fill2;
+                f->mid = (int16_t)sctx.imid;
+                f->side = (int16_t)sctx.iside;
+                f->itheta = itheta;
+                f->mbits = mbits;
+                f->sbits = sbits;
+                f->next_lowband2 = f->lowband ? f->lowband + N2 : 0;
+                f->rebalance = ctx->remaining_bits;
+                c->stage = 0;
+                c->N = N2;
+                c->B = B2;
+                c->LM = LM2;
+                if (mbits >= sbits) {
+                    f->stage = 1;
+                    c->X = f->X;
+                    c->b = mbits;
+                    c->lowband = f->lowband;
+                    c->gain = (int16_t)c_mul16_p15(f->gain, f->mid);
+                    c->fill = fill2;
+                } else {
+                    f->stage = 3;
+                    c->X = f->Y;
+                    c->b = sbits;
+                    c->lowband = f->next_lowband2;
+                    c->gain = (int16_t)c_mul16_p15(f->gain, f->side);
+                    c->fill = fill2 >> B2;
+                }
+                sp++;
+                continue;
+            }
+            ret = quant_partition_leaf(ctx, f->X, f->N, f->b, f->B, f->lowband, f->LM, f->gain, f->fill);
+            sp--;
+            continue;
+        }
+        if (f->stage == 1 || f->stage == 3) {
+            c->stage = 0;
+            c->N = f->N;
+            c->B = f->B;
+            c->LM = f->LM;
+            if (f->stage == 1) {            // mid half done: rebalance, then the side half
+                f->cm = ret;
+                int32_t rebalance = f->mbits - (f->rebalance - ctx->remaining_bits);
+                if (rebalance > 3 << 3 && f->itheta != 0) f->sbits += rebalance - (3 << 3);
+                c->X = f->Y;
+                c->b = f->sbits;
+                c->lowband = f->next_lowband2;
+                c->gain = (int16_t)c_mul16_p15(f->gain, f->side);
+                c->fill = f->fill >> f->B;
+                f->stage = 2;
+            } else {                        // side half done: rebalance, then the mid half
+                f->cm = ret << (f->B0 >> 1);
+                int32_t rebalance = f->sbits - (f->rebalance - ctx->remaining_bits);
+                if (rebalance > 3 << 3 && f->itheta != 16384) f->mbits += rebalance - (3 << 3);
+                c->X = f->X;
+                c->b = f->mbits;
+                c->lowband = f->lowband;
+                c->gain = (int16_t)c_mul16_p15(f->gain, f->mid);
+                c->fill = f->fill;
+                f->stage = 4;
+            }
+            sp++;
+            continue;
+        }
+        ret = f->stage == 2 ? f->cm | (ret << (f->B0 >> 1)) : f->cm | ret;
+        sp--;
     }
+    return ret;
 }
 
 // celt/bands.c quant_band (decoder, resynth always on)
@@ -1274,7 +1346,7 @@ DNI unsigned quant_band(BandCtx *ctx, int16_t *X, int N, int b, int B, int16_t *
     N_B0 = N_B;
     if (B0 > 1 && lowband)
         deinterleave_hadamard(lowband, N_B >> recombine, B0 << recombine, longBlocks, ctx->w->tmp);
-    cm = quant_partition_lm(ctx, X, N, b, B, lowband, LM, gain, fill);
+    cm = quant_partition(ctx, X, N, b, B, lowband, LM, gain, fill);
     if (B0 > 1) interleave_hadamard(X, N_B >> recombine, B0 << recombine, longBlocks, ctx->w->tmp);
     N_B = N_B0;
     B = B0;
@@ -2081,7 +2153,9 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
             }
         }
     }
+    PHASE_BEGIN(t_ce);
     unquant_coarse_energy(start, end, oldBandE, intra_ener, dec, C, LM);
+    PHASE_END(PH_CELT_COARSE, t_ce, L.id);
     int32_t *tf_res = w->tf_res;
     tf_decode(start, end, isTransient, tf_res, LM, dec);
     tell = rd_tell(dec);
@@ -2114,14 +2188,20 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
     int intensity = 0, dual_stereo = 0;
     int32_t balance;
     int32_t *pulses = w->pulses, *fine_quant = w->fine_quant, *fine_priority = w->fine_priority;
+    PHASE_BEGIN(t_al);
     int codedBands = clt_compute_allocation(start, end, offsets, cap, alloc_trim, &intensity, &dual_stereo, bits,
                                             &balance, pulses, fine_quant, fine_priority, C, LM, dec);
+    PHASE_END(PH_CELT_ALLOC, t_al, L.id);
     unquant_fine_energy(start, end, oldBandE, fine_quant, dec, C);
+    PHASE_BEGIN(t_sh);
     for (int c = 0; c < CC; c++) lshift_copy(L, st->decode_mem[c], CELT_DEC_BUF - N + CELT_OVERLAP, N);
+    PHASE_END(PH_CELT_SHIFT, t_sh, L.id);
     int16_t *X = w->X;
+    PHASE_BEGIN(t_qb);
     quant_all_bands_dec(L, start, end, X, C == 2 ? X + N : 0, w->collapse_masks, pulses, shortBlocks,
                         spread_decision, dual_stereo, intensity, tf_res, len * (8 << 3) - anti_collapse_rsv,
                         balance, dec, LM, codedBands, &st->rng, st->disable_inv, w);
+    PHASE_END(PH_CELT_BANDS, t_qb, L.id);
     int anti_collapse_on = 0;
     if (anti_collapse_rsv > 0) anti_collapse_on = (int)rd_bits(dec, 1);
     unquant_energy_finalise(start, end, oldBandE, fine_quant, fine_priority, len * 8 - rd_tell(dec), dec, C);
@@ -2131,7 +2211,10 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
         for (int i = 0; i < C * CELT_NB; i++) oldBandE[i] = -28672;   // -QCONST16(28.f, DB_SHIFT)
     if (st->prefilter_and_fold) prefilter_and_fold(st, N, w);
     lsync(L);
+    PHASE_BEGIN(t_sy);
     celt_synthesis(L, w, X, out_syn, oldBandE, start, effEnd, C, CC, isTransient, LM, silence);
+    PHASE_END(PH_CELT_SYNTH, t_sy, L.id);
+    PHASE_BEGIN(t_cb);
     for (int c = 0; c < CC; c++) {
         st->postfilter_period = imax(st->postfilter_period, 15);
         st->postfilter_period_old = imax(st->postfilter_period_old, 15);
@@ -2144,6 +2227,7 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
                         st->postfilter_tapset, postfilter_tapset, T_celt_window, CELT_OVERLAP);
     }
     lsync(L);
+    PHASE_END(PH_CELT_COMB, t_cb, L.id);
     st->postfilter_period_old = st->postfilter_period;
     st->postfilter_gain_old = st->postfilter_gain;
     st->postfilter_tapset_old = st->postfilter_tapset;
@@ -2179,7 +2263,9 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
         }
     }
     st->rng = dec->rng;
+    PHASE_BEGIN(t_de);
     deemphasis(L, out_syn[0], out_syn[1], pcm, N, CC, st->preemph_memD, accum);
+    PHASE_END(PH_CELT_DEEMPH, t_de, L.id);
     st->loss_duration = 0;
     st->prefilter_and_fold = 0;
     if (rd_tell(dec) > 8 * len) return -3;   // OPUS_INTERNAL_ERROR

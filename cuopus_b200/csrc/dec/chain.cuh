@@ -129,7 +129,7 @@ struct ChainResult {
     int32_t stop;          // 0, or the first negative opus_decode return
     uint32_t samples;      // samples per channel decoded
     uint32_t final_range;  // OPUS_GET_FINAL_RANGE after the last packet
-    uint32_t cycles;       // device clock cycles spent on the chain (0 on the host)
+    uint32_t time_us;      // microseconds the chain took on the device (0 on the host)
 };
 
 struct ChainSlot {         // per resident decoder group, in global memory
@@ -151,7 +151,9 @@ struct KeepWindow {
             int cnt = (int)(hi - lo) * channels;
             const int16_t *src = frame + (lo - pos) * channels;
             int16_t *dst = out + (lo - trim) * channels;
+            PHASE_BEGIN(t_kc);
             LFOR((*L), i, 0, cnt) dst[i] = src[i];
+            PHASE_END(PH_KEEP_COPY, t_kc, L->id);
         }
         lsync(*L);
         pos += (uint64_t)n;
@@ -161,10 +163,15 @@ struct KeepWindow {
 // Decode one chain.  pkt_nsamp / pkt_rng (optional) receive per-packet sample
 // counts and final ranges; `out` may be null (decode only).
 // `stage` (device only, may be null) stages the packets in shared memory.
+// fec = 1 turns on in-band FEC: a lost (empty) packet followed by a non-empty
+// one is decoded as opus_decode(next packet, 5760, decode_fec = 1), which
+// conceals the same 5760 samples a lost packet always yields but takes the
+// last frame's worth from the next packet's FEC (LBRR) data; the next packet
+// is then decoded normally.
 DNI void decode_chain(Lanes L, ChainSlot *slot, const uint8_t *data, const uint64_t *off,
                       const uint32_t *len, uint32_t first, uint32_t npkts, int channels, int16_t *out,
                       uint64_t trim, uint64_t keep, uint32_t *pkt_nsamp, uint32_t *pkt_rng, ChainResult *res,
-                      PacketStage *stage)
+                      PacketStage *stage, int fec)
 {
     OpusDec *st = &slot->dec;
     opus_init(st, channels);
@@ -186,6 +193,8 @@ DNI void decode_chain(Lanes L, ChainSlot *slot, const uint8_t *data, const uint6
     for (uint32_t k = 0; k < npkts; k++) {
         uint64_t p = (uint64_t)first + k;
         const uint8_t *pk = data + off[p];
+        int32_t n = (int32_t)len[p];
+        int use_fec = fec && n == 0 && k + 1 < npkts && len[p + 1] > 0;
 #ifdef __CUDA_ARCH__
         if (stage) {
             int b = (int)(k & 1u);
@@ -194,7 +203,13 @@ DNI void decode_chain(Lanes L, ChainSlot *slot, const uint8_t *data, const uint6
             if (cur && stage_ready(L, *stage, b)) pk = stage->buf + b * STAGE_BUF + ((uintptr_t)pk & 15);
         }
 #endif
-        int ret = opus_decode_packet(L, st, pk, (int32_t)len[p], slot->frame_buf, &slot->scratch, win);
+        PHASE_BEGIN(t_pk);
+        if (use_fec) {   // the next packet, read in place (its staged copy is still in flight)
+            pk = data + off[p + 1];
+            n = (int32_t)len[p + 1];
+        }
+        int ret = opus_decode_packet(L, st, pk, n, slot->frame_buf, &slot->scratch, win, use_fec);
+        PHASE_END(PH_PACKET, t_pk, L.id);
         lsync(L);   // every lane is done with this packet's buffer before it is refilled
         if (ret < 0) {
             stop = ret;

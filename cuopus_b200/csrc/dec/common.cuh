@@ -66,6 +66,31 @@ DFN void lsync(const Lanes &L)
 #define LFOR(L, i, start, end) for (int i = (start) + (L).id; i < (end); i += (L).n)
 #endif
 
+// Stage timers of the diagnostic build (CUO_PHASE_TIMERS, libcuopus_phases.so):
+// the first lane of each group adds the clock cycles a decoder stage took to
+// that stage's device counter (cuopus_phase_read).  Other builds compile them
+// to nothing.  Stage numbers: PH_* below.
+enum {
+    PH_PACKET = 0, PH_SILK_INDICES, PH_SILK_PULSES, PH_SILK_PARAMS, PH_SILK_CORE, PH_SILK_PLC, PH_SILK_CNG,
+    PH_SILK_STEREO, PH_SILK_RESAMPLE, PH_CELT_COARSE, PH_CELT_ALLOC, PH_CELT_SHIFT, PH_CELT_BANDS,
+    PH_CELT_SYNTH, PH_CELT_COMB, PH_CELT_DEEMPH, PH_KEEP_COPY, PH_COUNT
+};
+#if defined(CUO_PHASE_TIMERS) && defined(__CUDA_ARCH__)
+__device__ void cuo_phase_add(int stage, long long cycles);
+#define PHASE_BEGIN(v) long long v = clock64()
+#define PHASE_END(k, v, lane)                                                                        \
+    do {                                                                                             \
+        if ((lane) == 0) cuo_phase_add((k), clock64() - (v));                                        \
+    } while (0)
+#else
+#define PHASE_BEGIN(v) \
+    do {               \
+    } while (0)
+#define PHASE_END(k, v, lane) \
+    do {                      \
+    } while (0)
+#endif
+
 // Sum of v over the lanes of the group with wrap-around 32-bit adds (so the
 // order of the terms does not change the result); every lane gets the total.
 DFN int32_t lsum(const Lanes &L, int32_t v)

@@ -178,10 +178,12 @@ DNI void smooth_fade(Lanes L, const int16_t *in1, const int16_t *in2, int16_t *o
     lsync(L);
 }
 
-// src/opus_decoder.c opus_decode_frame (decode_fec = 0).  D is the recursion depth.
+// src/opus_decoder.c opus_decode_frame (:237-668).  D is the recursion depth;
+// fec = 1 decodes the SILK layer's in-band FEC (LBRR) frames of `data` and
+// conceals the CELT layer.
 template <int D>
 DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16_t *pcm, int frame_size,
-                   OpusScratch *w)
+                   OpusScratch *w, int fec)
 {
     const int F20 = 960, F10 = 480, F5 = 240, F2_5 = 120;
     const int C = st->channels;
@@ -214,7 +216,7 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
         if (audiosize > F20) {
             if constexpr (D == 0) {
                 do {
-                    int ret = opus_frame<1>(L, st, 0, 0, pcm, imin(audiosize, F20), w);
+                    int ret = opus_frame<1>(L, st, 0, 0, pcm, imin(audiosize, F20), w, 0);
                     if (ret < 0) return ret;
                     pcm += ret * C;
                     audiosize -= ret;
@@ -236,7 +238,7 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
     if (transition && mode == MODE_CELT_ONLY) {
         if constexpr (D == 0) {
             pcm_transition = w->pcm_transition;
-            opus_frame<1>(L, st, 0, 0, pcm_transition, imin(F5, audiosize), w);
+            opus_frame<1>(L, st, 0, 0, pcm_transition, imin(F5, audiosize), w, 0);
         }
     }
     if (audiosize > frame_size) return OPUS_BAD_ARG;
@@ -257,7 +259,7 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
                 st->DecControl.internalSampleRate = 16000;
             }
         }
-        int lost_flag = data == 0 ? 1 : 0;
+        int lost_flag = data == 0 ? 1 : (fec ? 2 : 0);
         int decoded_samples = 0;
         do {
             int first_frame = decoded_samples == 0;
@@ -279,7 +281,7 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
     }
 
     int start_band = 0;
-    if (mode != MODE_CELT_ONLY && data != 0 && rd_tell(&dec) + 17 + 20 * (mode == MODE_HYBRID) <= 8 * len) {
+    if (!fec && mode != MODE_CELT_ONLY && data != 0 && rd_tell(&dec) + 17 + 20 * (mode == MODE_HYBRID) <= 8 * len) {
         if (mode == MODE_HYBRID) redundancy = rd_bit_logp(&dec, 12);
         else redundancy = 1;
         if (redundancy) {
@@ -300,7 +302,7 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
     if (transition && mode != MODE_CELT_ONLY) {
         if constexpr (D == 0) {
             pcm_transition = w->pcm_transition;
-            opus_frame<1>(L, st, 0, 0, pcm_transition, imin(F5, audiosize), w);
+            opus_frame<1>(L, st, 0, 0, pcm_transition, imin(F5, audiosize), w, 0);
         }
     }
     if (bandwidth) {
@@ -325,7 +327,8 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
     if (mode != MODE_SILK_ONLY) {
         int celt_frame_size = imin(F20, frame_size);
         if (mode != st->prev_mode && st->prev_mode > 0 && !st->prev_redundancy) celt_reset(&st->celt);
-        celt_ret = celt_decode(L, &st->celt, data, len, pcm, celt_frame_size, data ? &dec : 0, celt_accum,
+        celt_ret = celt_decode(L, &st->celt, fec ? 0 : data, len, pcm, celt_frame_size, (data && !fec) ? &dec : 0,
+                               celt_accum,
                                &w->celt);
     } else {
         const uint8_t silence[2] = {0xFF, 0xFF};
@@ -385,25 +388,38 @@ DFN int packet_nb_samples(const uint8_t *data, int32_t len)
     return samples;
 }
 
-// src/opus_decoder.c opus_decode_native (decode_fec 0, not self-delimited,
+// Concealment of n samples per channel (src/opus_decoder.c:715-729, the
+// len == 0 branch of opus_decode_native), emitted frame by frame.
+template <class Emit>
+DFN int conceal_samples(Lanes L, OpusDec *st, int n, int16_t *frame_buf, OpusScratch *w, Emit &emit)
+{
+    int pcm_count = 0;
+    do {
+        int ret = opus_frame<0>(L, st, 0, 0, frame_buf, n - pcm_count, w, 0);
+        if (ret < 0) return ret;
+        emit(frame_buf, ret);
+        pcm_count += ret;
+    } while (pcm_count < n);
+    return pcm_count;
+}
+
+// src/opus_decoder.c opus_decode_native (:670-811; not self-delimited,
 // frame_size = MAX_PACKET_SAMPLES).  `emit(frame_pcm, n)` receives each decoded
 // frame (n samples per channel, interleaved) so the caller can place it; the
-// frame buffer is reused for the next frame.
+// frame buffer is reused for the next frame.  fec = 1 is decode_fec = 1: the
+// packet is the one after a lost packet, and the lost packet's audio is
+// concealed up to the last frame, which comes from the packet's FEC data
+// (:745-779).
 template <class Emit>
 DFN int opus_decode_packet(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16_t *frame_buf,
-                           OpusScratch *w, Emit &emit)
+                           OpusScratch *w, Emit &emit, int fec)
 {
     const int frame_size = MAX_PACKET_SAMPLES;
     if (len == 0 || data == 0) {
-        int pcm_count = 0;
-        do {
-            int ret = opus_frame<0>(L, st, 0, 0, frame_buf, frame_size - pcm_count, w);
-            if (ret < 0) return ret;
-            emit(frame_buf, ret);
-            pcm_count += ret;
-        } while (pcm_count < frame_size);
-        st->last_packet_duration = pcm_count;
-        return pcm_count;
+        int ret = conceal_samples(L, st, frame_size, frame_buf, w, emit);
+        if (ret < 0) return ret;
+        st->last_packet_duration = ret;
+        return ret;
     }
     if (len < 0) return OPUS_BAD_ARG;
     int packet_mode = toc_mode(data[0]);
@@ -415,6 +431,31 @@ DFN int opus_decode_packet(Lanes L, OpusDec *st, const uint8_t *data, int32_t le
     int count = packet_parse(data, len, size, &offset);
     if (count < 0) return count;
     data += offset;
+    if (fec) {
+        if (frame_size < packet_frame_size || packet_mode == MODE_CELT_ONLY || st->mode == MODE_CELT_ONLY) {
+            int ret = conceal_samples(L, st, frame_size, frame_buf, w, emit);
+            if (ret < 0) return ret;
+            st->last_packet_duration = ret;
+            return ret;
+        }
+        int duration_copy = st->last_packet_duration;
+        if (frame_size - packet_frame_size != 0) {
+            int ret = conceal_samples(L, st, frame_size - packet_frame_size, frame_buf, w, emit);
+            if (ret < 0) {
+                st->last_packet_duration = duration_copy;
+                return ret;
+            }
+        }
+        st->mode = packet_mode;
+        st->bandwidth = packet_bandwidth;
+        st->frame_size = packet_frame_size;
+        st->stream_channels = packet_stream_channels;
+        int ret = opus_frame<0>(L, st, data, size[0], frame_buf, packet_frame_size, w, 1);
+        if (ret < 0) return ret;
+        emit(frame_buf, ret);
+        st->last_packet_duration = frame_size;
+        return frame_size;
+    }
     if (count * packet_frame_size > frame_size) return OPUS_BUFFER_TOO_SMALL;
     st->mode = packet_mode;
     st->bandwidth = packet_bandwidth;
@@ -422,7 +463,7 @@ DFN int opus_decode_packet(Lanes L, OpusDec *st, const uint8_t *data, int32_t le
     st->stream_channels = packet_stream_channels;
     int nb_samples = 0;
     for (int i = 0; i < count; i++) {
-        int ret = opus_frame<0>(L, st, data, size[i], frame_buf, frame_size - nb_samples, w);
+        int ret = opus_frame<0>(L, st, data, size[i], frame_buf, frame_size - nb_samples, w, 0);
         if (ret < 0) return ret;
         emit(frame_buf, ret);
         data += size[i];

@@ -1232,15 +1232,25 @@ DNI void silk_decode_frame(Lanes L, SilkChan *c, RangeDec *rd, int16_t *pOut, in
     ctrl->LTP_scale_Q14 = 0;
     if (lostFlag == LOSS_NONE || (lostFlag == LOSS_LBRR && c->LBRR_flags[c->nFramesDecoded] == 1)) {
         int16_t *pulses = w->pulses;
+        PHASE_BEGIN(t_ix);
         silk_decode_indices(c, rd, c->nFramesDecoded, lostFlag, condCoding);
+        PHASE_END(PH_SILK_INDICES, t_ix, L.id);
+        PHASE_BEGIN(t_pu);
         silk_decode_pulses(rd, pulses, c->indices.signalType, c->indices.quantOffsetType, c->frame_length);
+        PHASE_END(PH_SILK_PULSES, t_pu, L.id);
+        PHASE_BEGIN(t_pa);
         silk_decode_parameters(c, ctrl, condCoding);
+        PHASE_END(PH_SILK_PARAMS, t_pa, L.id);
+        PHASE_BEGIN(t_co);
         silk_decode_core(L, c, ctrl, pOut, pulses, w);
+        PHASE_END(PH_SILK_CORE, t_co, L.id);
         int mv = c->ltp_mem_length - c->frame_length;
         lshift_copy(L, c->outBuf, mv, c->frame_length);
         LFOR(L, i, 0, c->frame_length) c->outBuf[mv + i] = pOut[i];
         lsync(L);
+        PHASE_BEGIN(t_pl);
         silk_plc(L, c, ctrl, pOut, 0, w);
+        PHASE_END(PH_SILK_PLC, t_pl, L.id);
         c->lossCnt = 0;
         c->prevSignalType = c->indices.signalType;
         c->first_frame_after_reset = 0;
@@ -1251,7 +1261,9 @@ DNI void silk_decode_frame(Lanes L, SilkChan *c, RangeDec *rd, int16_t *pOut, in
         LFOR(L, i, 0, c->frame_length) c->outBuf[mv + i] = pOut[i];
         lsync(L);
     }
+    PHASE_BEGIN(t_cn);
     silk_cng(c, ctrl, pOut, Lf, w);
+    PHASE_END(PH_SILK_CNG, t_cn, L.id);
     silk_plc_glue_frames(c, pOut, Lf);
     c->lagPrev = ctrl->pitchL[c->nb_subfr - 1];
     *pN = Lf;
@@ -1418,7 +1430,9 @@ DNI int silk_decode(Lanes L, SilkDec *dec, SilkDecControl *ctl, int lostFlag, in
         cs[n].nFramesDecoded++;
     }
     if (ctl->nChannelsAPI == 2 && ctl->nChannelsInternal == 2) {
+        PHASE_BEGIN(t_st);
         silk_stereo_ms_to_lr(L, &dec->sStereo, tmp[0], tmp[1], MS_pred_Q13, cs[0].fs_kHz, nSamplesOutDec);
+        PHASE_END(PH_SILK_STEREO, t_st, L.id);
     } else {
         int16_t m0 = dec->sStereo.sMid[0], m1 = dec->sStereo.sMid[1];
         int16_t n0 = tmp[0][nSamplesOutDec], n1 = tmp[0][nSamplesOutDec + 1];
@@ -1432,7 +1446,9 @@ DNI int silk_decode(Lanes L, SilkDec *dec, SilkDecControl *ctl, int lostFlag, in
     int16_t *rs_out = ctl->nChannelsAPI == 2 ? w->rs_out : samplesOut;
     int nres = imin(ctl->nChannelsAPI, ctl->nChannelsInternal);
     for (int n = 0; n < nres; n++) {
+        PHASE_BEGIN(t_rs);
         silk_resample(L, &cs[n].resampler_state, rs_out, &tmp[n][1], nSamplesOutDec, w->rs_buf);
+        PHASE_END(PH_SILK_RESAMPLE, t_rs, L.id);
         if (ctl->nChannelsAPI == 2) {
             LFOR(L, i, 0, *nSamplesOut) samplesOut[n + 2 * i] = rs_out[i];
             lsync(L);

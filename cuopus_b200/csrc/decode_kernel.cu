@@ -137,6 +137,7 @@ extern "C" int cuopus_decode_batch_noalloc(const cuopus_batch *b, void *cuda_str
     a.nchains = b->nchains;
     a.width = width;
     a.use_queue = 0;
+    a.fec = b->fec != 0;
     k_decode_chains<<<blocks, block, 0, st>>>(a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return noalloc_err(errbuf, errcap, 2, "decode launch", e);
@@ -144,3 +145,30 @@ extern "C" int cuopus_decode_batch_noalloc(const cuopus_batch *b, void *cuda_str
     if (e != cudaSuccess) return noalloc_err(errbuf, errcap, 2, "decode", e);
     return 0;
 }
+
+#ifdef CUO_PHASE_TIMERS
+#include "../../include/cuopus_phases.h"
+
+// Stage timers of the diagnostic build (libcuopus_phases.so only): cycles per
+// decoder stage summed over every chain of every launch since the last reset.
+namespace cuo {
+__device__ unsigned long long g_phase_cycles[PH_COUNT];
+__device__ void cuo_phase_add(int stage, long long cycles)
+{
+    atomicAdd(&g_phase_cycles[stage], (unsigned long long)cycles);
+}
+} // namespace cuo
+
+extern "C" int cuopus_phase_count(void) { return cuo::PH_COUNT; }
+
+extern "C" int cuopus_phase_read(uint64_t *out)
+{
+    return cudaMemcpyFromSymbol(out, cuo::g_phase_cycles, sizeof(cuo::g_phase_cycles)) == cudaSuccess ? 0 : 2;
+}
+
+extern "C" int cuopus_phase_reset(void)
+{
+    static const unsigned long long zero[cuo::PH_COUNT] = {};
+    return cudaMemcpyToSymbol(cuo::g_phase_cycles, zero, sizeof zero) == cudaSuccess ? 0 : 2;
+}
+#endif

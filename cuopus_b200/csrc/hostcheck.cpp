@@ -25,6 +25,7 @@ struct hc_job {
     uint32_t *pkt_nsamp, *pkt_rng;
     cuo::ChainResult *res;
     int nchains;
+    int fec;
     int next;
     pthread_mutex_t mu;
 };
@@ -47,7 +48,7 @@ static void *hc_worker(void *arg)
         cuo::decode_chain(L, slot, j->data, j->off, j->len, j->first[c], j->npkts[c], j->channels[c],
                           j->pcm ? j->pcm + j->pcm_off[c] : nullptr, j->trim ? j->trim[c] : 0,
                           j->keep ? j->keep[c] : (uint64_t)-1 / 4, j->pkt_nsamp ? j->pkt_nsamp + r : nullptr,
-                          j->pkt_rng ? j->pkt_rng + r : nullptr, &j->res[c], nullptr);
+                          j->pkt_rng ? j->pkt_rng + r : nullptr, &j->res[c], nullptr, j->fec);
     }
     free(slot);
     return nullptr;
@@ -55,12 +56,13 @@ static void *hc_worker(void *arg)
 
 // Same layout as the oracle's oref_decode_chains, plus per-chain channels and
 // keep windows (trim/keep may be null: keep everything).  res: 4 words per chain.
-int hc_decode_chains(const uint8_t *data, const uint64_t *off, const uint32_t *len, const uint32_t *first,
-                     const uint32_t *npkts, const int32_t *channels, int nchains, int16_t *pcm,
-                     const uint64_t *pcm_off, const uint64_t *trim, const uint64_t *keep, const uint64_t *rec_off,
-                     uint32_t *pkt_nsamp, uint32_t *pkt_rng, void *res, int nthreads)
+int hc_decode_chains_fec(const uint8_t *data, const uint64_t *off, const uint32_t *len, const uint32_t *first,
+                         const uint32_t *npkts, const int32_t *channels, int nchains, int16_t *pcm,
+                         const uint64_t *pcm_off, const uint64_t *trim, const uint64_t *keep, const uint64_t *rec_off,
+                         uint32_t *pkt_nsamp, uint32_t *pkt_rng, void *res, int nthreads, int fec)
 {
     hc_job j;
+    j.fec = fec;
     j.data = data; j.off = off; j.len = len; j.first = first; j.npkts = npkts; j.channels = channels;
     j.pcm = pcm; j.pcm_off = pcm_off; j.trim = trim; j.keep = keep; j.rec_off = rec_off;
     j.pkt_nsamp = pkt_nsamp; j.pkt_rng = pkt_rng; j.res = (cuo::ChainResult *)res;
@@ -78,6 +80,15 @@ int hc_decode_chains(const uint8_t *data, const uint64_t *off, const uint32_t *l
     for (int t = 0; t < started; t++) pthread_join(th[t], nullptr);
     pthread_mutex_destroy(&j.mu);
     return 0;
+}
+
+int hc_decode_chains(const uint8_t *data, const uint64_t *off, const uint32_t *len, const uint32_t *first,
+                     const uint32_t *npkts, const int32_t *channels, int nchains, int16_t *pcm,
+                     const uint64_t *pcm_off, const uint64_t *trim, const uint64_t *keep, const uint64_t *rec_off,
+                     uint32_t *pkt_nsamp, uint32_t *pkt_rng, void *res, int nthreads)
+{
+    return hc_decode_chains_fec(data, off, len, first, npkts, channels, nchains, pcm, pcm_off, trim, keep, rec_off,
+                                pkt_nsamp, pkt_rng, res, nthreads, 0);
 }
 
 unsigned long hc_slot_bytes(void) { return sizeof(cuo::ChainSlot); }

@@ -44,6 +44,7 @@ struct DecodeArgs {
     int use_queue;
     int stage;                  // packets staged in shared memory (STAGE_BYTES per group)
     int scalar;                 // one active lane per group (the reference kernel's slot layout)
+    int fec;                    // in-band FEC for lost packets (decode_chain)
 };
 
 // Shared memory a block of `block` threads at `width` lanes per chain uses for
@@ -65,6 +66,14 @@ cudaError_t decode_kernel_launch(const DecodeArgs &a, int blocks, int block, cud
 cudaError_t resample_into(const int16_t *in, long long avail, long long n_out, float *out, cudaStream_t st);
 
 #ifdef CUO_DECODE_KERNEL_TU
+// The device's global nanosecond timer (PTX %globaltimer).
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // Resident 128-thread blocks per SM the register allocation is sized for.
 #ifndef CUO_MIN_BLOCKS
 #define CUO_MIN_BLOCKS 1
@@ -106,13 +115,13 @@ __global__ void __launch_bounds__(128, CUO_MIN_BLOCKS) k_decode_chains(DecodeArg
         }
         if (pos >= a.nchains) break;
         int c = a.order ? (int)a.order[pos] : pos;
-        long long t0 = clock64();
+        unsigned long long t0 = globaltimer_ns();
         decode_chain(L, slot, a.data, a.off, a.len, a.first[c], a.npkts[c], a.channels[c],
                      a.out ? a.out + a.out_off[c] : nullptr, a.trim[c], a.keep[c],
                      a.pkt_nsamp ? a.pkt_nsamp + a.rec_off[c] : nullptr,
-                     a.pkt_rng ? a.pkt_rng + a.rec_off[c] : nullptr, &a.res[c], stage);
-        long long t1 = clock64();
-        if (L.id == 0) a.res[c].cycles = (uint32_t)min(t1 - t0, 0xffffffffLL);
+                     a.pkt_rng ? a.pkt_rng + a.rec_off[c] : nullptr, &a.res[c], stage, a.fec);
+        unsigned long long us = (globaltimer_ns() - t0) / 1000ull;
+        if (L.id == 0) a.res[c].time_us = (uint32_t)(us < 1 ? 1 : us > 0xffffffffull ? 0xffffffffull : us);
     }
 }
 #endif

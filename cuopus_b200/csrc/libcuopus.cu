@@ -359,6 +359,7 @@ int decode_batch(const cuopus_batch *b, cudaStream_t st, float *kernel_ms, Err &
     a.width = width;
     a.use_queue = b->schedule == 1;
     a.scalar = b->scalar != 0;
+    a.fec = b->fec != 0;
     CK(cudaEventRecord(G.ev0, st));
     if (b->graph) {
         if ((rc = launch_graph(a, blocks, block, st, err))) return rc;

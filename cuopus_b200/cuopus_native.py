@@ -51,7 +51,7 @@ class Batch(ctypes.Structure):
                 ("pkt_rng", ctypes.c_void_p), ("res", ctypes.c_void_p), ("nchains", ctypes.c_int32),
                 ("width", ctypes.c_int32), ("schedule", ctypes.c_int32), ("max_groups", ctypes.c_int32),
                 ("order", ctypes.c_void_p), ("block", ctypes.c_int32), ("graph", ctypes.c_int32),
-                ("scalar", ctypes.c_int32)]
+                ("scalar", ctypes.c_int32), ("fec", ctypes.c_int32)]
 
 
 _lib = None
@@ -353,3 +353,40 @@ def last_arena_overflow() -> bool:
 
 def release_workspaces():
     _load().cuopus_release_workspaces()
+
+
+# Decoder stages timed by the diagnostic build (libcuopus_phases.so), in the
+# order of the device counters.  "packet" spans the whole of one packet's
+# decode and contains the others; "keep_copy" (the PCM write) runs inside it.
+PHASE_NAMES = ("packet", "silk_indices", "silk_pulses", "silk_params", "silk_core", "silk_plc", "silk_cng",
+               "silk_stereo", "silk_resample", "celt_coarse", "celt_alloc", "celt_shift", "celt_bands",
+               "celt_synth", "celt_comb", "celt_deemph", "keep_copy")
+
+
+def phases_lib_path():
+    """Path of the diagnostic build with the decoder's stage timers."""
+    return os.path.join(_HERE, "lib", "libcuopus_phases.so")
+
+
+def phase_reset():
+    """Zero the stage counters (diagnostic build only)."""
+    lib = _load()
+    if not hasattr(lib, "cuopus_phase_reset"):
+        raise CuopusError(3, "the loaded library has no stage timers (load %s via CUOPUS_LIB)" % phases_lib_path())
+    if lib.cuopus_phase_reset():
+        raise CuopusError(2, "cuopus_phase_reset failed")
+
+
+def phase_cycles():
+    """Device clock cycles per decoder stage since phase_reset(), summed over
+    the first lane of every chain (dict name -> cycles)."""
+    lib = _load()
+    if not hasattr(lib, "cuopus_phase_read"):
+        raise CuopusError(3, "the loaded library has no stage timers (load %s via CUOPUS_LIB)" % phases_lib_path())
+    n = int(lib.cuopus_phase_count())
+    if n != len(PHASE_NAMES):
+        raise CuopusError(3, "library has %d stage counters, this module knows %d" % (n, len(PHASE_NAMES)))
+    buf = (ctypes.c_uint64 * n)()
+    if lib.cuopus_phase_read(buf):
+        raise CuopusError(2, "cuopus_phase_read failed")
+    return dict(zip(PHASE_NAMES, (int(v) for v in buf)))

@@ -97,7 +97,8 @@ int cuopus_decode_i16_multi(const uint8_t *const *oggs, const size_t *ns, int nf
  * kernel) as a CUDA graph, captured on first use for these arguments.
  * pkt_nsamp / pkt_rng (device, may be NULL) receive per-packet sample counts
  * and final ranges at rec_off[c] + k.  res: 4 x uint32 per chain
- * {stop, samples, final_range, cycles}.  kernel_ms (host, may be NULL)
+ * {stop, samples, final_range, time_us}: time_us is the chain's decode time in
+ * microseconds (device global timer, at least 1).  kernel_ms (host, may be NULL)
  * receives the decode kernel time measured with events on the stream. */
 typedef struct cuopus_batch {
     const uint8_t *data;
@@ -123,6 +124,11 @@ typedef struct cuopus_batch {
     int32_t graph;
     int32_t scalar;      /* 1: only the first lane of each group decodes (lane-split loops run
                             serially): the reference kernel's slot layout, for comparison */
+    int32_t fec;         /* 1: in-band FEC.  A lost (empty) packet followed by a non-empty one
+                            is decoded as opus_decode(next, 5760, decode_fec = 1): the same
+                            5760 concealed samples as without FEC, the last frame's worth
+                            rebuilt from the next packet's LBRR data.  0: the reference's
+                            protocol (decode_fec = 0 for every packet). */
 } cuopus_batch;
 
 int cuopus_decode_batch(const cuopus_batch *b, void *cuda_stream, float *kernel_ms, char *errbuf, size_t errcap);
@@ -157,7 +163,7 @@ int cuopus_autotune(const cuopus_batch *b, const int32_t *widths, int nwidths, c
 
 /* ---- Extension: learned cost model of the queue schedule (no counterpart in
  * the reference).  An FP32 MLP 16 -> 64 -> 64 -> 1 (ReLU) predicts a chain's
- * log decode cycles from 16 features of its packets' TOC bytes; chains are
+ * log decode time from 16 features of its packets' TOC bytes; chains are
  * queued longest first by the prediction.  It orders work only: decoded
  * samples do not depend on it.  All buffers are device pointers. */
 #define CUOPUS_MLP_FEATURES 16

@@ -67,9 +67,13 @@ def ref_lib():
             ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
             ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_int,
             ctypes.POINTER(ctypes.c_int)]
+        lib.oref_encode_opts.restype = ctypes.c_int
+        lib.oref_encode_opts.argtypes = lib.oref_encode.argtypes + [ctypes.c_int] * 3
         lib.oref_decode_chains.restype = ctypes.c_int
         lib.oref_decode_chains.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_int, ctypes.c_int] + \
             [ctypes.c_void_p] * 7 + [ctypes.c_int]
+        lib.oref_decode_chains_fec.restype = ctypes.c_int
+        lib.oref_decode_chains_fec.argtypes = lib.oref_decode_chains.argtypes + [ctypes.c_int]
         lib.oref_version.restype = ctypes.c_char_p
         _lib = lib
     return _lib
@@ -161,8 +165,11 @@ class Seg:
     force_channels: int = OPUS_AUTO
 
 
-def encode(pcm_i16, channels, segs, application=APP_AUDIO, complexity=10, vbr=1):
-    """Encode interleaved int16 pcm (n*channels) -> (list of packets, preskip)."""
+def encode(pcm_i16, channels, segs, application=APP_AUDIO, complexity=10, vbr=1, inband_fec=0, loss_perc=0,
+           dtx=0):
+    """Encode interleaved int16 pcm (n*channels) -> (list of packets, preskip).
+    inband_fec / loss_perc / dtx: OPUS_SET_INBAND_FEC, OPUS_SET_PACKET_LOSS_PERC
+    and OPUS_SET_DTX (all 0 for the corpora)."""
     lib = ref_lib()
     pcm = np.ascontiguousarray(pcm_i16, dtype=np.int16)
     n = pcm.size // channels
@@ -173,9 +180,9 @@ def encode(pcm_i16, channels, segs, application=APP_AUDIO, complexity=10, vbr=1)
     out = np.zeros(cap, dtype=np.uint8)
     lens = np.zeros(max_pkts, dtype=np.uint32)
     pre = ctypes.c_int(0)
-    np_ = lib.oref_encode(pcm.ctypes.data, n, channels, arr, len(segs), application,
-                          complexity, vbr, out.ctypes.data, cap, lens.ctypes.data,
-                          max_pkts, ctypes.byref(pre))
+    np_ = lib.oref_encode_opts(pcm.ctypes.data, n, channels, arr, len(segs), application,
+                               complexity, vbr, out.ctypes.data, cap, lens.ctypes.data,
+                               max_pkts, ctypes.byref(pre), inband_fec, loss_perc, dtx)
     if np_ < 0:
         raise RuntimeError("oref_encode failed: %d" % np_)
     pkts, w = [], 0
@@ -308,7 +315,9 @@ def make_stream(spec):
     elif kind == "mixed":
         x, _ = _signal(rng, n, ch)
         segs = _mixed_segments(rng, n, ch)
-        pkts, pre = encode(x, ch, segs, APP_AUDIO, complexity=spec.get("complexity", 5))
+        pkts, pre = encode(x, ch, segs, APP_AUDIO, complexity=spec.get("complexity", 5),
+                           inband_fec=spec.get("inband_fec", 0), loss_perc=spec.get("loss_perc", 0),
+                           dtx=spec.get("dtx", 0))
     elif kind == "long":
         x = to_i16(synth("speech", n, rng))
         segs, pos, j = [], 0, 0

@@ -35,6 +35,14 @@ def toc_samples48(pkt: bytes) -> int:
     return QMS[pkt[0] >> 3] * 12 * nf
 
 
+def decode_capacity48(pkt: bytes) -> int:
+    """Samples per channel opus_decode(..., frame_size=5760, 0) can return for
+    this packet: the TOC's count, or 5760 for an empty packet (a lost packet:
+    opus_decode_native conceals until frame_size is filled,
+    src/opus_decoder.c:715-729 of the vendored libopus)."""
+    return 5760 if len(pkt) == 0 else toc_samples48(pkt)
+
+
 class DemuxError(ValueError):
     pass
 

@@ -24,8 +24,9 @@ def flatten(packets):
     return blob, off, lens
 
 
-def decode_chains(packets, chains, channels, nthreads=None, want_pcm=True):
+def decode_chains(packets, chains, channels, nthreads=None, want_pcm=True, fec=0):
     """chains: sequence of (first, npkts[, trim, keep]) over `packets`.
+    fec=1: in-band FEC for a lost (empty) packet followed by a non-empty one.
 
     Returns dict(pcm=list of int16 arrays (interleaved), nsamp=list of uint32
     arrays, rng=list of uint32 arrays, status=int32 array, samples=uint64 array)."""
@@ -49,12 +50,12 @@ def decode_chains(packets, chains, channels, nthreads=None, want_pcm=True):
     rng = np.zeros(max(nrec, 1), dtype=np.uint32)
     status = np.zeros(max(nch, 1), dtype=np.int32)
     samples = np.zeros(max(nch, 1), dtype=np.uint64)
-    rc = lib.oref_decode_chains(
+    rc = lib.oref_decode_chains_fec(
         blob.ctypes.data, off.ctypes.data, lens.ctypes.data, first.ctypes.data,
         npk.ctypes.data, nch, channels,
         pcm.ctypes.data if want_pcm else None, pcm_off.ctypes.data, rec_off.ctypes.data,
         nsamp.ctypes.data, rng.ctypes.data, status.ctypes.data, samples.ctypes.data,
-        nthreads or (os.cpu_count() or 1))
+        nthreads or (os.cpu_count() or 1), fec)
     if rc != 0:
         raise RuntimeError("oref_decode_chains failed to start threads")
     out = dict(status=status[:nch], samples=samples[:nch], pcm=[], nsamp=[], rng=[])
@@ -69,5 +70,5 @@ def decode_chains(packets, chains, channels, nthreads=None, want_pcm=True):
 
 
 def _toc(p):
-    from .ogg_port import toc_samples48
-    return toc_samples48(p)
+    from .ogg_port import decode_capacity48
+    return decode_capacity48(p)

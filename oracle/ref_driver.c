@@ -11,9 +11,13 @@
  *    against libopus in harness2.cu:200-253.  Per packet it records the sample
  *    count and OPUS_GET_FINAL_RANGE; per chain the stop status and sample total.
  *    Chains run on a pthread pool (dynamic assignment) so the same entry point
- *    is the timed CPU baseline.
+ *    is the timed CPU baseline.  oref_decode_chains_fec adds in-band FEC: a
+ *    lost (empty) packet followed by a non-empty one is decoded as
+ *    opus_decode(next packet, 5760, decode_fec=1), the next packet then
+ *    normally (the use of decode_fec in src/opus_demo.c, with the chain
+ *    protocol's frame size).
  *
- * 2. oref_encode: the corpus encoder.  Drives the vendored encoder frame by
+ * 2. oref_encode / oref_encode_opts: the corpus encoder.  Drives the vendored encoder frame by
  *    frame at 48 kHz with per-segment forced mode / bandwidth / frame size /
  *    bitrate (OPUS_SET_FORCE_MODE is the private request 11002 of
  *    src/opus_private.h:141; per-frame switching follows the idea of
@@ -47,6 +51,7 @@ typedef struct {
     uint32_t *pkt_rng;          /* per record (may be NULL) */
     int32_t *chain_status;      /* per chain: 0 or first negative opus_decode return */
     uint64_t *chain_samples;    /* per chain: samples per channel decoded */
+    int fec;                    /* in-band FEC for lost packets */
     volatile int next;
     pthread_mutex_t mu;
 } oref_job;
@@ -71,8 +76,10 @@ static void *oref_worker(void *arg)
                 uint64_t p = (uint64_t)j->first[c] + k;
                 int16_t *out = j->pcm ? j->pcm + j->pcm_off[c] + total * (uint64_t)j->channels
                                       : scratch;
-                int ret = opus_decode(dec, j->data + j->off[p], (opus_int32)j->len[p], out,
-                                      OREF_MAX_PKT_SAMPLES, 0);
+                int use_fec = j->fec && j->len[p] == 0 && k + 1 < j->npkts[c] && j->len[p + 1] > 0;
+                uint64_t q = use_fec ? p + 1 : p;
+                int ret = opus_decode(dec, j->data + j->off[q], (opus_int32)j->len[q], out,
+                                      OREF_MAX_PKT_SAMPLES, use_fec);
                 uint64_t r = j->rec_off ? j->rec_off[c] + k : 0;
                 if (ret < 0) {
                     status = ret;
@@ -95,6 +102,12 @@ static void *oref_worker(void *arg)
     return NULL;
 }
 
+int oref_decode_chains_fec(const uint8_t *data, const uint64_t *off, const uint32_t *len,
+                           const uint32_t *first, const uint32_t *npkts, int nchains,
+                           int channels, int16_t *pcm, const uint64_t *pcm_off,
+                           const uint64_t *rec_off, uint32_t *pkt_nsamp, uint32_t *pkt_rng,
+                           int32_t *chain_status, uint64_t *chain_samples, int nthreads, int fec);
+
 /* Decode nchains chains; returns 0, or -1 when a thread could not start. */
 int oref_decode_chains(const uint8_t *data, const uint64_t *off, const uint32_t *len,
                        const uint32_t *first, const uint32_t *npkts, int nchains,
@@ -102,8 +115,19 @@ int oref_decode_chains(const uint8_t *data, const uint64_t *off, const uint32_t 
                        const uint64_t *rec_off, uint32_t *pkt_nsamp, uint32_t *pkt_rng,
                        int32_t *chain_status, uint64_t *chain_samples, int nthreads)
 {
+    return oref_decode_chains_fec(data, off, len, first, npkts, nchains, channels, pcm, pcm_off, rec_off,
+                                  pkt_nsamp, pkt_rng, chain_status, chain_samples, nthreads, 0);
+}
+
+int oref_decode_chains_fec(const uint8_t *data, const uint64_t *off, const uint32_t *len,
+                           const uint32_t *first, const uint32_t *npkts, int nchains,
+                           int channels, int16_t *pcm, const uint64_t *pcm_off,
+                           const uint64_t *rec_off, uint32_t *pkt_nsamp, uint32_t *pkt_rng,
+                           int32_t *chain_status, uint64_t *chain_samples, int nthreads, int fec)
+{
     oref_job j;
     memset(&j, 0, sizeof(j));
+    j.fec = fec;
     j.data = data; j.off = off; j.len = len; j.first = first; j.npkts = npkts;
     j.rec_off = rec_off; j.pcm_off = pcm_off; j.nchains = nchains; j.channels = channels;
     j.pcm = pcm; j.pkt_nsamp = pkt_nsamp; j.pkt_rng = pkt_rng;
@@ -139,19 +163,35 @@ typedef struct {
  * into out (capacity out_cap bytes) and their lengths into pkt_len (capacity
  * max_pkts).  Returns the packet count, or a negative value on error.
  * *preskip receives OPUS_GET_LOOKAHEAD. */
+int oref_encode_opts(const int16_t *pcm, int64_t n, int channels, const oref_seg *segs,
+                     int nsegs, int application, int complexity, int vbr,
+                     uint8_t *out, uint64_t out_cap, uint32_t *pkt_len, int max_pkts,
+                     int *preskip, int inband_fec, int loss_perc, int dtx);
+
 int oref_encode(const int16_t *pcm, int64_t n, int channels, const oref_seg *segs,
                 int nsegs, int application, int complexity, int vbr,
                 uint8_t *out, uint64_t out_cap, uint32_t *pkt_len, int max_pkts,
                 int *preskip)
+{
+    return oref_encode_opts(pcm, n, channels, segs, nsegs, application, complexity, vbr, out, out_cap, pkt_len,
+                            max_pkts, preskip, 0, 0, 0);
+}
+
+/* oref_encode with in-band FEC (LBRR frames, sized for loss_perc % loss) and
+ * DTX switched on or off. */
+int oref_encode_opts(const int16_t *pcm, int64_t n, int channels, const oref_seg *segs,
+                     int nsegs, int application, int complexity, int vbr,
+                     uint8_t *out, uint64_t out_cap, uint32_t *pkt_len, int max_pkts,
+                     int *preskip, int inband_fec, int loss_perc, int dtx)
 {
     int err = 0;
     OpusEncoder *enc = opus_encoder_create(48000, channels, application, &err);
     if (!enc || err) return -1000 + err;
     opus_encoder_ctl(enc, OPUS_SET_COMPLEXITY(complexity));
     opus_encoder_ctl(enc, OPUS_SET_VBR(vbr));
-    opus_encoder_ctl(enc, OPUS_SET_INBAND_FEC(0));
-    opus_encoder_ctl(enc, OPUS_SET_DTX(0));
-    opus_encoder_ctl(enc, OPUS_SET_PACKET_LOSS_PERC(0));
+    opus_encoder_ctl(enc, OPUS_SET_INBAND_FEC(inband_fec));
+    opus_encoder_ctl(enc, OPUS_SET_DTX(dtx));
+    opus_encoder_ctl(enc, OPUS_SET_PACKET_LOSS_PERC(loss_perc));
     int la = 0;
     opus_encoder_ctl(enc, OPUS_GET_LOOKAHEAD(&la));
     if (preskip) *preskip = la;

@@ -8,7 +8,7 @@ def device_batch(packets_list, chains_list, channels_list):
     records).  Returns (Batch, tensors to keep alive, meta dict)."""
     import torch
     from cuopus_b200 import cuopus_native as cn
-    from oracle.ogg_port import toc_samples48
+    from oracle.ogg_port import decode_capacity48 as toc_samples48
     blob, off, lens, first, npk, chans, trim, keep, cap = [], [], [], [], [], [], [], [], []
     base_pkt = base_byte = 0
     for pk, chs, ch in zip(packets_list, chains_list, channels_list):
@@ -67,7 +67,7 @@ def run_device_batch(b, meta, width=32, schedule=1, order=None, block=0, graph=0
 
 
 def run_batch(packets_list, chains_list, channels_list, width=32, schedule=0, order=None, max_groups=0,
-              records=True):
+              records=True, fec=0):
     """Decode chains of several streams in one launch.
 
     packets_list[s]: list of packets of stream s; chains_list[s]: (first, npkts, trim, keep) over it;
@@ -93,7 +93,7 @@ def run_batch(packets_list, chains_list, channels_list, width=32, schedule=0, or
         base_pkt += len(pk)
     n = len(first)
     cap = []
-    from oracle.ogg_port import toc_samples48
+    from oracle.ogg_port import decode_capacity48 as toc_samples48
     allp = [p for pk in packets_list for p in pk]
     for i in range(n):
         cap.append(sum(toc_samples48(allp[first[i] + k]) for k in range(npk[i])))
@@ -130,6 +130,7 @@ def run_batch(packets_list, chains_list, channels_list, width=32, schedule=0, or
         b.rec_off, b.pkt_nsamp, b.pkt_rng = d_roff.data_ptr(), d_ns.data_ptr(), d_rg.data_ptr()
     b.res = d_res.data_ptr()
     b.nchains, b.width, b.schedule, b.max_groups = n, width, schedule, max_groups
+    b.fec = fec
     order_arr = None
     if order is not None:
         order_arr = np.ascontiguousarray(np.array(order, np.uint32))
@@ -146,6 +147,6 @@ def run_batch(packets_list, chains_list, channels_list, width=32, schedule=0, or
         r0 = int(rec_off[i])
         chains.append(dict(pcm=out[o:o + keep[i] * chans[i]], nsamp=ns[r0:r0 + npk[i]], rng=rg[r0:r0 + npk[i]],
                            stop=int(res[i, 0]), samples=int(res[i, 1].view(np.uint32) if hasattr(res[i, 1], 'view') else res[i, 1]),
-                           final_range=int(np.uint32(res[i, 2])), cycles=int(np.uint32(res[i, 3])),
+                           final_range=int(np.uint32(res[i, 2])), time_us=int(np.uint32(res[i, 3])),
                            trim=trim[i], keep=keep[i], cap=cap[i]))
     return chains, ms

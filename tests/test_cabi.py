@@ -71,3 +71,22 @@ def test_no_cpu_fallback_on_the_decode_path():
                                    ctypes.byref(out_len), None, err, 256)
     assert rc == 2, (rc, err.value)
     assert out_len.value == 0
+
+
+PHASES_HEADER = os.path.join(ROOT, "include", "cuopus_phases.h")
+PHASES_LIB = os.path.join(ROOT, "cuopus_b200", "lib", "libcuopus_phases.so")
+
+
+def test_stage_timer_build_exports_both_headers():
+    """libcuopus_phases.so is the product library plus the stage timers; the
+    product library itself carries no timers."""
+    src = re.sub(r"/\*.*?\*/", "", open(PHASES_HEADER).read(), flags=re.S)
+    timer_names = sorted(set(re.findall(r"\b(cuopus_[a-z0-9_]+)\s*\(", src)))
+    assert timer_names == ["cuopus_phase_count", "cuopus_phase_read", "cuopus_phase_reset"]
+    lib = ctypes.CDLL(PHASES_LIB)
+    missing = [n for n in declared() + timer_names if not hasattr(lib, n)]
+    assert not missing, missing
+    from cuopus_b200 import cuopus_native as cn
+    assert lib.cuopus_phase_count() == len(cn.PHASE_NAMES)
+    out = subprocess.run(["nm", "-D", "--defined-only", LIB], capture_output=True, text=True).stdout
+    assert "cuopus_phase_read" not in out

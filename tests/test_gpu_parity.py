@@ -136,3 +136,95 @@ def test_i16_stereo_and_mono(cuda):
         want, wch, _ = pipeline.i16(d)
         assert ch == wch
         assert np.array_equal(t.cpu().numpy(), want)
+
+
+def _lossy(packets, seed, p_lost, p_dtx):
+    """Some packets empty (lost: concealment), some cut to the TOC byte (DTX)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for p in packets:
+        u = rng.random()
+        if u < p_lost:
+            out.append(b"")
+        elif u < p_lost + p_dtx and (p[0] & 3) == 0:
+            out.append(p[:1])
+        else:
+            out.append(p)
+    return out
+
+
+@pytest.mark.parametrize("width", [32, 8])
+def test_concealment_matches_libopus(cuda, width):
+    """Lost and DTX packets in SILK / hybrid / CELT streams, mono and stereo:
+    SILK PLC and CNG, CELT PLC and the transitions around them, bit-exact."""
+    from gpu_util import run_batch
+    pk, chs, nch = [], [], []
+    for s in range(4):
+        d = corpus.make_stream(dict(kind="mixed", seed=21 + s, seconds=4.0, channels=1 + s % 2))
+        ix = ogg_port.demux(d)
+        p = _lossy(ix["packets"], 21 + s, 0.12, 0.08)
+        pk.append(p)
+        chs.append([(0, len(p), 0, 1 << 40)] + [(i, min(20, len(p) - i), 0, 1 << 40) for i in range(0, len(p), 20)])
+        nch.append(ix["channels"])
+    res, _ = run_batch(pk, chs, nch, width=width, schedule=1, order=None)
+    k = 0
+    for s in range(len(pk)):
+        _check(res[k:k + len(chs[s])], pk[s], [(c[0], c[1], 0, r["keep"]) for c, r in
+                                               zip(chs[s], res[k:k + len(chs[s])])], nch[s], True)
+        k += len(chs[s])
+
+
+def test_damaged_packets_stop_like_libopus(cuda):
+    """Truncated and bit-flipped packets: same stop status, per-packet counts,
+    final ranges and samples as libopus up to the first error."""
+    from gpu_util import run_batch
+    rng = np.random.default_rng(5)
+    pk, nch = [], []
+    for s in range(6):
+        ix = ogg_port.demux(corpus.make_stream(dict(kind="mixed", seed=31 + s, seconds=3.0, channels=1 + s % 2)))
+        p = list(ix["packets"])
+        for i in range(s % 5, len(p), 5 + s):
+            b = bytearray(p[i])
+            if i % 3 == 0 and len(b) > 3:
+                b = b[: len(b) // 2]
+            elif len(b) > 2:
+                b[int(rng.integers(1, len(b)))] ^= 1 << int(rng.integers(0, 8))
+            p[i] = bytes(b)
+        pk.append(p)
+        nch.append(ix["channels"])
+    res, _ = run_batch(pk, [[(0, len(p), 0, 1 << 40)] for p in pk], nch, width=32, schedule=1)
+    for s in range(len(pk)):
+        ref = ref_decode.decode_chains(pk[s], [(0, len(pk[s]))], nch[s])
+        g = res[s]
+        assert g["stop"] == int(ref["status"][0])
+        assert np.array_equal(g["nsamp"], ref["nsamp"][0]) and np.array_equal(g["rng"], ref["rng"][0])
+        n = int(ref["samples"][0]) * nch[s]
+        assert g["samples"] == int(ref["samples"][0])
+        assert np.array_equal(g["pcm"][:n], ref["pcm"][0])
+
+
+@pytest.mark.parametrize("fec", [1, 0])
+def test_inband_fec_matches_libopus(cuda, fec):
+    """Streams with in-band FEC (LBRR) and DTX, 15 % of packets lost: with
+    cuopus_batch.fec = 1 a lost packet is rebuilt from the next packet's LBRR
+    frames exactly as libopus's decode_fec = 1 does; with fec = 0 the same
+    streams conceal like the reference's protocol."""
+    from gpu_util import run_batch
+    pk, chs, nch = [], [], []
+    for seed, ch in [(42, 2), (44, 2), (45, 1), (48, 1), (49, 1)]:
+        d = corpus.make_stream(dict(kind="mixed", seed=seed, seconds=5.0, channels=ch, inband_fec=1, loss_perc=25,
+                                    dtx=1))
+        ix = ogg_port.demux(d)
+        p = _lossy(ix["packets"], seed, 0.15, 0.0)
+        pk.append(p)
+        chs.append([(0, len(p), 0, 1 << 40)] + [(i, min(25, len(p) - i), 0, 1 << 40) for i in range(0, len(p), 25)])
+        nch.append(ix["channels"])
+    res, _ = run_batch(pk, chs, nch, width=32, schedule=1, fec=fec)
+    k = 0
+    for s in range(len(pk)):
+        ref = ref_decode.decode_chains(pk[s], [c[:2] for c in chs[s]], nch[s], fec=fec)
+        for i, g in enumerate(res[k:k + len(chs[s])]):
+            assert g["stop"] == int(ref["status"][i]) == 0
+            assert np.array_equal(g["nsamp"], ref["nsamp"][i]) and np.array_equal(g["rng"], ref["rng"][i])
+            assert np.array_equal(g["pcm"], ref["pcm"][i]), "stream %d chain %d" % (s, i)
+        k += len(chs[s])

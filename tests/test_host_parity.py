@@ -173,14 +173,14 @@ def test_range_decoder_gate_schedules(hc):
         assert [int(x) for x in o2] == case["wide"]
 
 
-def host_decode(hc, packets, chains, ch, nthreads=4):
+def host_decode(hc, packets, chains, ch, nthreads=4, fec=0):
     """Decode chains with the host build; returns per chain (pcm, nsamp, rng, stop, samples)."""
     blob, off, lens = ref_decode.flatten(packets)
     n = len(chains)
     first = np.array([c[0] for c in chains], np.uint32)
     npk = np.array([c[1] for c in chains], np.uint32)
     chans = np.full(n, ch, np.int32)
-    cap = np.array([sum(ogg_port.toc_samples48(packets[int(first[i]) + k]) for k in range(int(npk[i])))
+    cap = np.array([sum(ogg_port.decode_capacity48(packets[int(first[i]) + k]) for k in range(int(npk[i])))
                     for i in range(n)], np.uint64)
     pcm_off = np.zeros(n, np.uint64)
     pcm_off[1:] = np.cumsum(cap[:-1] * ch)
@@ -191,8 +191,8 @@ def host_decode(hc, packets, chains, ch, nthreads=4):
     rg = np.zeros_like(ns)
     res = np.zeros(4 * n, np.uint32)
     P = lambda a: ctypes.c_void_p(a.ctypes.data)
-    hc.hc_decode_chains(P(blob), P(off), P(lens), P(first), P(npk), P(chans), n, P(pcm), P(pcm_off), None, None,
-                        P(rec), P(ns), P(rg), P(res), nthreads)
+    hc.hc_decode_chains_fec(P(blob), P(off), P(lens), P(first), P(npk), P(chans), n, P(pcm), P(pcm_off), None,
+                            None, P(rec), P(ns), P(rg), P(res), nthreads, fec)
     res = res.reshape(-1, 4)
     out = []
     for i in range(n):
@@ -279,3 +279,68 @@ def test_host_decoder_damaged_packets_match_libopus(hc):
     assert stop == int(ref["status"][0])
     assert np.array_equal(ns, ref["nsamp"][0]) and np.array_equal(rg, ref["rng"][0])
     assert np.array_equal(pcm, ref["pcm"][0])
+
+
+def _lossy(packets, seed, p_lost, p_dtx):
+    """Packets with some replaced by an empty packet (lost: concealment) and
+    some cut to their TOC byte (a DTX frame)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for p in packets:
+        u = rng.random()
+        if u < p_lost:
+            out.append(b"")
+        elif u < p_lost + p_dtx and (p[0] & 3) == 0:
+            out.append(p[:1])
+        else:
+            out.append(p)
+    return out
+
+
+@pytest.mark.parametrize("seed", [21, 22, 23, 24])
+def test_host_decoder_concealment_matches_libopus(hc, seed):
+    """Lost and DTX packets in SILK, hybrid and CELT streams, mono and stereo:
+    SILK PLC / CNG, CELT PLC (pitch search, LPC, IIR) and the transition
+    frames around them match libopus sample for sample."""
+    try:
+        corpus.ref_lib()
+    except OSError as e:
+        pytest.skip(str(e))
+    d = corpus.make_stream(dict(kind="mixed", seed=seed, seconds=4.0, channels=1 + seed % 2))
+    ix = ogg_port.demux(d)
+    pk = _lossy(ix["packets"], seed, 0.12, 0.08)
+    assert any(len(p) == 0 for p in pk) and any(len(p) == 1 for p in pk)
+    chains = [(0, len(pk))] + [(i, min(20, len(pk) - i)) for i in range(0, len(pk), 20)]
+    ref = ref_decode.decode_chains(pk, chains, ix["channels"])
+    got = host_decode(hc, pk, chains, ix["channels"])
+    for i in range(len(chains)):
+        pcm, ns, rg, stop, _ = got[i]
+        assert stop == int(ref["status"][i]), i
+        assert np.array_equal(ns, ref["nsamp"][i]) and np.array_equal(rg, ref["rng"][i]), i
+        assert np.array_equal(pcm, ref["pcm"][i]), i
+
+
+@pytest.mark.parametrize("seed,channels", [(42, 2), (44, 2), (45, 1), (48, 1), (49, 1)])
+def test_host_decoder_inband_fec_matches_libopus(hc, seed, channels):
+    """Streams encoded with in-band FEC (LBRR) and DTX, packets lost at random:
+    with FEC on, a lost packet is rebuilt from the next packet's LBRR frames
+    (opus_decode(next, 5760, decode_fec = 1)); every sample, count and final
+    range matches libopus, and FEC changes the output of some lost packets."""
+    try:
+        corpus.ref_lib()
+    except OSError as e:
+        pytest.skip(str(e))
+    d = corpus.make_stream(dict(kind="mixed", seed=seed, seconds=5.0, channels=channels, inband_fec=1,
+                                loss_perc=25, dtx=1))
+    ix = ogg_port.demux(d)
+    pk = _lossy(ix["packets"], seed, 0.15, 0.0)
+    chains = [(0, len(pk))] + [(i, min(25, len(pk) - i)) for i in range(0, len(pk), 25)]
+    ref = ref_decode.decode_chains(pk, chains, ix["channels"], fec=1)
+    ref0 = ref_decode.decode_chains(pk, chains[:1], ix["channels"], fec=0)
+    assert not np.array_equal(ref["pcm"][0], ref0["pcm"][0]), "no packet used its FEC data"
+    got = host_decode(hc, pk, chains, ix["channels"], fec=1)
+    for i in range(len(chains)):
+        pcm, ns, rg, stop, _ = got[i]
+        assert stop == int(ref["status"][i]), i
+        assert np.array_equal(ns, ref["nsamp"][i]) and np.array_equal(rg, ref["rng"][i]), i
+        assert np.array_equal(pcm, ref["pcm"][i]), i
