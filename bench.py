@@ -11,7 +11,8 @@ encoder (oracle/corpus.py), generated before anything is timed.
 A step is one decode of the whole batch.
   value      scheduled form: persistent grid pulling chains from a device work
              queue, longest first by the learned cost model, replayed as a CUDA
-             graph, width x block picked by the autotuner; packets and chain
+             graph, width x block and decoder groups per SM picked by the
+             autotuner; packets and chain
              tables already in HBM; CUDA-event time on the launching stream
   plain      the plain one-launch form on the same batch: one warp per chain,
              one launch, chains in index order (the reference kernel's layout)
@@ -301,16 +302,22 @@ def schedule_batch(cn, db, stream, args):
         info["order"] = "learned (MLP 16-64-64-1)"
         info["cost_model"] = {"train_s": round(time.time() - t0, 2), "loss_first": float(losses[0]),
                               "loss_last": float(losses[-1]), "r2_log_cycles": round(float(r2), 4)}
-    # autotune width x block on the scheduled form
-    width, block = args.width, args.block
+    # autotune width x block on the scheduled form, then the decoder groups per SM
+    width, block, max_groups = args.width, args.block, 0
+    sched = {"queue": 1, "static": 0, "plain": 2}[args.schedule]
     if not args.no_tune:
         b = db.batch(32, 1, order, 128, 1)
         width, block, table = cn.autotune(b, widths=(8, 16, 32), blocks=(64, 128), reps=1,
                                           stream=stream.cuda_stream)
         info["autotune"] = {"%dx%d" % k: (round(v, 1) if v else None) for k, v in table.items()}
-    sched = {"queue": 1, "static": 0, "plain": 2}[args.schedule]
+        if sched != 2:
+            b = db.batch(width, sched, order if sched == 1 else None, block, 1)
+            max_groups, occ = cn.autotune_occupancy(b, groups_per_sm=(0, 7, 6, 5, 4), reps=2,
+                                                    stream=stream.cuda_stream)
+            info["autotune_groups_per_sm"] = {str(k): (round(v, 1) if v else None) for k, v in occ.items()}
     b = db.batch(width, sched, order if sched == 1 else None, block, 1 if sched != 2 else 0)
-    info.update(width=width, block=block)
+    b.max_groups = max_groups
+    info.update(width=width, block=block, max_groups=max_groups)
     return b, info
 
 
@@ -398,12 +405,15 @@ def serve_bench(args, files, dev):
 def phases_report(args):
     """Split of the decoder's time between its stages, from the stage timers of
     the diagnostic build: one decode of the workload in the lane-split form
-    (the --width / --block given, packet-count order, queue schedule) and one
-    in the one-lane reference layout.  Prints one JSON line (not a bench line:
+    (the --width / --block given, packet-count order, queue schedule), one in
+    the one-lane layout with the same order and schedule, and one in the
+    one-lane reference layout (plain one-launch form, index order).  Prints one JSON line (not a bench line:
     the timers cost time of their own)."""
     import torch
     from cuopus_b200 import cuopus_native as cn
-    os.environ["CUOPUS_LIB"] = cn.phases_lib_path()     # before the library is first loaded
+    # before the library is first loaded; a CUOPUS_LIB already set must name a
+    # stage-timer build
+    os.environ.setdefault("CUOPUS_LIB", cn.phases_lib_path())
     from cuopus_b200 import costmodel
     torch.cuda.set_device(0)
     files, seg = load_inputs(args.workload, args.count)
@@ -414,6 +424,7 @@ def phases_report(args):
     # DeviceBatch.batch() keeps the order array of the latest batch alive only,
     # so each batch is made right before its use
     forms = {"lane_split": lambda: db.batch(args.width, 1, order, args.block, 0),
+             "one_lane_queue": lambda: db.batch(32, 1, order, 128, 0, scalar=1),
              "one_lane": lambda: db.batch(32, 2, None, 128, 0, scalar=1)}
     out = {"report": "decoder stage cycles", "workload": args.workload, "chains": db.n,
            "audio_s": round(db.audio_s, 1), "width": args.width, "block": args.block}

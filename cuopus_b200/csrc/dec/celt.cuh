@@ -46,7 +46,23 @@ struct CeltDec {
     int16_t oldBandE[2 * CELT_NB], oldLogE[2 * CELT_NB], oldLogE2[2 * CELT_NB], backgroundLogE[2 * CELT_NB];
 };
 
+// One frame of quant_partition's explicit stack (the state of one split level).
+struct QPFrame {
+    int16_t *X, *Y, *lowband, *next_lowband2;
+    int N, b, B, B0, LM, fill, mbits, sbits, itheta, stage;
+    int32_t rebalance;
+    int16_t gain, mid, side;
+    unsigned cm;
+};
+
+// Per lane group, in the decoder slot.  Besides the frame buffers it holds
+// what would otherwise be function-local arrays of the serial stages: every
+// lane of a group computes the same values, so one copy per group serves all
+// of them (a per-lane stack copy would multiply the memory these stages touch
+// by the group width).
 struct CeltScratch {
+    QPFrame qp[5];                    // quant_partition's split stack
+    int32_t bits1[CELT_NB], bits2[CELT_NB], thresh[CELT_NB], trim_offset[CELT_NB];   // allocation
     int16_t X[2 * 960];
     int32_t freq[960];
     int16_t norm[2 * 8 * 78];
@@ -332,11 +348,13 @@ DNI void denormalise_bands(Lanes L, const int16_t *X, int32_t *freq, const int16
 
 // celt/celt.c comb_filter (in place when y == x): the IIR recursion over lag T
 // is kept serial.
+// gains[3][3] of celt/celt.c (comb filter taps per tapset)
+TABC(int16_t, T_comb_gains[3][3]) = {{10048, 7112, 4248}, {15200, 8784, 0}, {26208, 3280, 0}};
+
 DNI void comb_filter(int32_t *y, int32_t *x, int T0, int T1, int N, int16_t g0, int16_t g1, int tapset0,
                      int tapset1, const int16_t *window, int overlap)
 {
-    // gains[3][3] of celt/celt.c
-    const int16_t gains[3][3] = {{10048, 7112, 4248}, {15200, 8784, 0}, {26208, 3280, 0}};
+    const int16_t (*gains)[3] = T_comb_gains;
     if (g0 == 0 && g1 == 0) {
         if (x != y) for (int i = 0; i < N; i++) y[i] = x[i];
         return;
@@ -391,7 +409,7 @@ DNI void comb_filter(int32_t *y, int32_t *x, int T0, int T1, int N, int16_t g0, 
 DNI void comb_filter_lanes(Lanes L, int32_t *y, int32_t *x, int T0, int T1, int N, int16_t g0, int16_t g1,
                            int tapset0, int tapset1, const int16_t *window, int overlap)
 {
-    const int16_t gains[3][3] = {{10048, 7112, 4248}, {15200, 8784, 0}, {26208, 3280, 0}};
+    const int16_t (*gains)[3] = T_comb_gains;
     lsync(L);
     if (g0 == 0 && g1 == 0) {
         if (x != y) {
@@ -756,10 +774,10 @@ DNI int interp_bits2pulses(int start, int end, int skip_start, const int32_t *bi
 
 DNI int clt_compute_allocation(int start, int end, const int32_t *offsets, const int32_t *cap, int alloc_trim,
                                int *intensity, int *dual_stereo, int32_t total, int32_t *balance, int32_t *pulses,
-                               int32_t *ebits, int32_t *fine_priority, int C, int LM, RangeDec *ec)
+                               int32_t *ebits, int32_t *fine_priority, int C, int LM, RangeDec *ec, CeltScratch *w)
 {
     const int16_t *eB = T_celt_eBands;
-    int32_t bits1[CELT_NB], bits2[CELT_NB], thresh[CELT_NB], trim_offset[CELT_NB];
+    int32_t *bits1 = w->bits1, *bits2 = w->bits2, *thresh = w->thresh, *trim_offset = w->trim_offset;
     total = max32(total, 0);
     int skip_start = start;
     int skip_rsv = total >= 1 << 3 ? 1 << 3 : 0;
@@ -911,9 +929,8 @@ DNI void exp_rotation1(int16_t *X, int len, int stride, int16_t c, int16_t s)
 // celt/vq.c exp_rotation, dir = -1 (decoder)
 DNI void exp_rotation_dec(int16_t *X, int len, int stride, int K, int spread)
 {
-    const int SPREAD_FACTOR[3] = {15, 10, 5};
     if (2 * K >= len || spread == SPREAD_NONE) return;
-    int factor = SPREAD_FACTOR[spread - 1];
+    int factor = spread == 1 ? 15 : spread == 2 ? 10 : 5;   // SPREAD_FACTOR[spread - 1] = {15, 10, 5}
     int16_t gain = (int16_t)c_mul32_q31(c_mul16(32767, len), c_rcp(len + factor * K));
     int16_t theta = (int16_t)(c_mul16_q15(gain, gain) >> 1);
     int16_t c = c_cos_norm(theta);
@@ -1040,9 +1057,12 @@ struct SplitCtx {
     int inv, imid, iside, delta, itheta, qalloc;
 };
 
+// exp2_table8 of celt/bands.c compute_qn
+TABC(int16_t, T_exp2_table8[8]) = {16384, 17866, 19483, 21247, 23170, 25267, 27554, 30048};
+
 DFN int compute_qn(int N, int b, int offset, int pulse_cap, int stereo)
 {
-    const int16_t exp2_table8[8] = {16384, 17866, 19483, 21247, 23170, 25267, 27554, 30048};
+    const int16_t *exp2_table8 = T_exp2_table8;
     int N2 = 2 * N - 1;
     if (stereo && N == 2) N2--;
     int qb = (b + N2 * offset) / N2;
@@ -1189,18 +1209,10 @@ DNI unsigned quant_partition_leaf(BandCtx *ctx, int16_t *X, int N, int b, int B,
 // when the mid half went first, 3 / 4 when the side half did; the bit
 // rebalancing between the halves and the collapse-mask combination happen at
 // those points, in libopus's order.
-struct QPFrame {
-    int16_t *X, *Y, *lowband, *next_lowband2;
-    int N, b, B, B0, LM, fill, mbits, sbits, itheta, stage;
-    int32_t rebalance;
-    int16_t gain, mid, side;
-    unsigned cm;
-};
-
 DNI unsigned quant_partition(BandCtx *ctx, int16_t *X, int N, int b, int B, int16_t *lowband, int LM,
                              int16_t gain, int fill)
 {
-    QPFrame st[5];
+    QPFrame *st = ctx->w->qp;
     int sp = 0;
     st[0].X = X;
     st[0].N = N;
@@ -1310,13 +1322,17 @@ DNI unsigned quant_partition(BandCtx *ctx, int16_t *X, int N, int b, int B, int1
     return ret;
 }
 
+// bit_interleave_table / bit_deinterleave_table of celt/bands.c quant_band
+TABC(uint8_t, T_bit_interleave[16]) = {0, 1, 1, 1, 2, 3, 3, 3, 2, 3, 3, 3, 2, 3, 3, 3};
+TABC(uint8_t, T_bit_deinterleave[16]) = {0x00, 0x03, 0x0C, 0x0F, 0x30, 0x33, 0x3C, 0x3F,
+                                         0xC0, 0xC3, 0xCC, 0xCF, 0xF0, 0xF3, 0xFC, 0xFF};
+
 // celt/bands.c quant_band (decoder, resynth always on)
 DNI unsigned quant_band(BandCtx *ctx, int16_t *X, int N, int b, int B, int16_t *lowband, int LM,
                         int16_t *lowband_out, int16_t gain, int16_t *lowband_scratch, int fill)
 {
-    const uint8_t bit_interleave_table[16] = {0, 1, 1, 1, 2, 3, 3, 3, 2, 3, 3, 3, 2, 3, 3, 3};
-    const uint8_t bit_deinterleave_table[16] = {0x00, 0x03, 0x0C, 0x0F, 0x30, 0x33, 0x3C, 0x3F,
-                                                0xC0, 0xC3, 0xCC, 0xCF, 0xF0, 0xF3, 0xFC, 0xFF};
+    const uint8_t *bit_interleave_table = T_bit_interleave;
+    const uint8_t *bit_deinterleave_table = T_bit_deinterleave;
     int N0 = N, N_B = N, N_B0, B0 = B, time_divide = 0, recombine = 0;
     int longBlocks = B0 == 1;
     unsigned cm = 0;
@@ -2190,7 +2206,7 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
     int32_t *pulses = w->pulses, *fine_quant = w->fine_quant, *fine_priority = w->fine_priority;
     PHASE_BEGIN(t_al);
     int codedBands = clt_compute_allocation(start, end, offsets, cap, alloc_trim, &intensity, &dual_stereo, bits,
-                                            &balance, pulses, fine_quant, fine_priority, C, LM, dec);
+                                            &balance, pulses, fine_quant, fine_priority, C, LM, dec, w);
     PHASE_END(PH_CELT_ALLOC, t_al, L.id);
     unquant_fine_energy(start, end, oldBandE, fine_quant, dec, C);
     PHASE_BEGIN(t_sh);

@@ -39,6 +39,7 @@ struct OpusScratch {
     int16_t pcm_silk[2][480 * 2];       // per recursion depth, IMAX(F10, frame_size) * channels
     int16_t pcm_transition[240 * 2];
     int16_t redundant_audio[240 * 2];
+    int16_t sizes[48];                  // frame sizes of the packet being decoded
 };
 
 DNI void opus_init(OpusDec *st, int channels)
@@ -426,7 +427,7 @@ DFN int opus_decode_packet(Lanes L, OpusDec *st, const uint8_t *data, int32_t le
     int packet_bandwidth = toc_bandwidth(data[0]);
     int packet_frame_size = toc_samples_per_frame(data[0]);
     int packet_stream_channels = (data[0] & 0x4) ? 2 : 1;
-    int16_t size[48];
+    int16_t *size = w->sizes;
     int offset = 0;
     int count = packet_parse(data, len, size, &offset);
     if (count < 0) return count;

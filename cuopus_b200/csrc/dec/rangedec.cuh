@@ -151,10 +151,13 @@ DNI uint32_t rd_uint(RangeDec *d, uint32_t ft)
 
 DFN int rd_tell(const RangeDec *d) { return d->nbits_total - ilog(d->rng); }
 
+// correction thresholds of celt/entcode.c ec_tell_frac
+TABC(unsigned, T_tell_frac_corr[8]) = {35733, 38967, 42495, 46340, 50535, 55109, 60097, 65535};
+
 DFN uint32_t rd_tell_frac(const RangeDec *d)
 {
     // 1/8-bit resolution: a linear estimate corrected against fixed thresholds
-    const unsigned corr[8] = {35733, 38967, 42495, 46340, 50535, 55109, 60097, 65535};
+    const unsigned *corr = T_tell_frac_corr;
     uint32_t nbits = (uint32_t)d->nbits_total << 3;
     int l = ilog(d->rng);
     uint32_t r = d->rng >> (l - 16);

@@ -121,7 +121,23 @@ struct SilkDecControl {   // silk_DecControlStruct (decoder fields)
 };
 
 // Per-slot scratch of the SILK decoder (replaces the stack arrays of libopus).
+// Arrays of the serial SILK stages (NLSF decoding and NLSF2A, inverse
+// prediction gain, pulse counts and the shell split tree).  Every lane of a
+// group computes the same values, so they live once per group in the decoder
+// slot rather than once per lane on the stack.
+struct SilkWork {
+    int32_t A[16];                                        // silk_lpc_inv_pred_gain
+    int32_t cos_LSF_QA[16], P[9], Q[9], a32_QA1[16];      // silk_nlsf2a
+    int16_t ec_ix[16], res_Q10[16];                       // NLSF unpack / residuals
+    uint8_t pred_Q8[16];
+    int16_t pNLSF_Q15[16], pNLSF0_Q15[16];                // silk_decode_parameters
+    int32_t sum_pulses[20], nLshifts[20];                 // silk_decode_pulses
+    int16_t shell[14];                                    // shell split tree: p3[2], p2[4], p1[8]
+    uint8_t sign_icdf[2];
+};
+
 struct SilkScratch {
+    SilkWork sw;
     int16_t pulses[SILK_MAX_FRAME + 16];
     int16_t lbrr_pulses[SILK_MAX_FRAME + 16];
     int16_t sLTP[SILK_MAX_FRAME];
@@ -294,11 +310,10 @@ DFN void silk_bwexpander_32(int32_t *ar, int d, int32_t chirp_Q16)
 }
 
 // silk/LPC_inv_pred_gain.c (QA = 24); returns 0 when the filter is unstable
-DNI int32_t silk_lpc_inv_pred_gain(const int16_t *A_Q12, int order)
+DNI int32_t silk_lpc_inv_pred_gain(const int16_t *A_Q12, int order, int32_t *A)
 {
     const int32_t A_LIMIT = 16773022;   // SILK_FIX_CONST(0.99975, 24)
     const int32_t MIN_INVG = 107374;    // SILK_FIX_CONST(1 / MAX_PREDICTION_POWER_GAIN, 30)
-    int32_t A[16];
     int32_t DC = 0;
     for (int k = 0; k < order; k++) {
         DC += A_Q12[k];
@@ -378,13 +393,14 @@ DFN void silk_nlsf2a_poly(int32_t *out, const int32_t *cLSF, int dd)
     }
 }
 
-DNI void silk_nlsf2a(int16_t *a_Q12, const int16_t *NLSF, int d)
+// ordering16 / ordering10 of silk/NLSF2A.c
+TABC(uint8_t, T_nlsf2a_ord16[16]) = {0, 15, 8, 7, 4, 11, 12, 3, 2, 13, 10, 5, 6, 9, 14, 1};
+TABC(uint8_t, T_nlsf2a_ord10[10]) = {0, 9, 6, 3, 4, 5, 8, 1, 2, 7};
+
+DNI void silk_nlsf2a(int16_t *a_Q12, const int16_t *NLSF, int d, SilkWork *sw)
 {
-    // ordering16 / ordering10 of silk/NLSF2A.c
-    const uint8_t ord16[16] = {0, 15, 8, 7, 4, 11, 12, 3, 2, 13, 10, 5, 6, 9, 14, 1};
-    const uint8_t ord10[10] = {0, 9, 6, 3, 4, 5, 8, 1, 2, 7};
-    const uint8_t *ordering = d == 16 ? ord16 : ord10;
-    int32_t cos_LSF_QA[16], P[9], Q[9], a32_QA1[16];
+    const uint8_t *ordering = d == 16 ? T_nlsf2a_ord16 : T_nlsf2a_ord10;
+    int32_t *cos_LSF_QA = sw->cos_LSF_QA, *P = sw->P, *Q = sw->Q, *a32_QA1 = sw->a32_QA1;
     for (int k = 0; k < d; k++) {
         int32_t f_int = NLSF[k] >> 8;
         int32_t f_frac = NLSF[k] - shl32(f_int, 8);
@@ -402,7 +418,7 @@ DNI void silk_nlsf2a(int16_t *a_Q12, const int16_t *NLSF, int d)
         a32_QA1[d - k - 1] = wsub(Qtmp, Ptmp);
     }
     silk_lpc_fit(a_Q12, a32_QA1, 12, 17, d);
-    for (int i = 0; silk_lpc_inv_pred_gain(a_Q12, d) == 0 && i < 16; i++) {
+    for (int i = 0; silk_lpc_inv_pred_gain(a_Q12, d, sw->A) == 0 && i < 16; i++) {
         silk_bwexpander_32(a32_QA1, d, 65536 - shl32(2, i));
         for (int k = 0; k < d; k++) a_Q12[k] = (int16_t)s_rshift_round(a32_QA1[k], 5);
     }
@@ -467,10 +483,10 @@ DFN void silk_nlsf_unpack(int16_t *ec_ix, uint8_t *pred_Q8, const NlsfCB &cb, in
 }
 
 // silk/NLSF_decode.c
-DNI void silk_nlsf_decode(int16_t *pNLSF_Q15, const int8_t *NLSFIndices, const NlsfCB &cb)
+DNI void silk_nlsf_decode(int16_t *pNLSF_Q15, const int8_t *NLSFIndices, const NlsfCB &cb, SilkWork *sw)
 {
-    uint8_t pred_Q8[16];
-    int16_t ec_ix[16], res_Q10[16];
+    uint8_t *pred_Q8 = sw->pred_Q8;
+    int16_t *ec_ix = sw->ec_ix, *res_Q10 = sw->res_Q10;
     silk_nlsf_unpack(ec_ix, pred_Q8, cb, NLSFIndices[0]);
     int32_t out_Q10 = 0;
     for (int i = cb.order - 1; i >= 0; i--) {
@@ -607,7 +623,8 @@ DNI void silk_decoder_set_fs(SilkChan *c, int fs_kHz, int32_t fs_API_Hz)
 
 // ------------------------------------------------------------------ entropy decoding
 
-DNI void silk_decode_indices(SilkChan *c, RangeDec *rd, int FrameIndex, int decode_LBRR, int condCoding)
+DNI void silk_decode_indices(SilkChan *c, RangeDec *rd, int FrameIndex, int decode_LBRR, int condCoding,
+                             SilkWork *sw)
 {
     SilkIndices *ix = &c->indices;
     int Ix;
@@ -626,9 +643,8 @@ DNI void silk_decode_indices(SilkChan *c, RangeDec *rd, int FrameIndex, int deco
 
     NlsfCB cb = silk_nlsf_cb(c->LPC_order);
     ix->NLSFIndices[0] = (int8_t)rd_icdf(rd, &cb.CB1_iCDF[(ix->signalType >> 1) * cb.nVectors], 8);
-    int16_t ec_ix[16];
-    uint8_t pred_Q8[16];
-    silk_nlsf_unpack(ec_ix, pred_Q8, cb, ix->NLSFIndices[0]);
+    int16_t *ec_ix = sw->ec_ix;
+    silk_nlsf_unpack(ec_ix, sw->pred_Q8, cb, ix->NLSFIndices[0]);
     for (int i = 0; i < cb.order; i++) {
         Ix = rd_icdf(rd, &cb.ec_iCDF[ec_ix[i]], 8);
         if (Ix == 0) Ix -= rd_icdf(rd, T_silk_NLSF_EXT_iCDF, 8);
@@ -677,9 +693,9 @@ DFN void silk_shell_split(int16_t *p1, int16_t *p2, RangeDec *rd, int p, const u
 }
 
 // silk/shell_coder.c silk_shell_decoder: binary split tree over 16 pulses
-DNI void silk_shell_decoder(int16_t *p0, RangeDec *rd, int pulses4)
+DNI void silk_shell_decoder(int16_t *p0, RangeDec *rd, int pulses4, int16_t *tree)
 {
-    int16_t p3[2], p2[4], p1[8];
+    int16_t *p3 = tree, *p2 = tree + 2, *p1 = tree + 6;
     const uint8_t *t0 = T_silk_shell_code_table0, *t1 = T_silk_shell_code_table1,
                   *t2 = T_silk_shell_code_table2, *t3 = T_silk_shell_code_table3;
     silk_shell_split(&p3[0], &p3[1], rd, pulses4, t3);
@@ -701,9 +717,9 @@ DNI void silk_shell_decoder(int16_t *p0, RangeDec *rd, int pulses4)
 
 // silk/decode_pulses.c + code_signs.c silk_decode_signs
 DNI void silk_decode_pulses(RangeDec *rd, int16_t *pulses, int signalType, int quantOffsetType,
-                            int frame_length)
+                            int frame_length, SilkWork *sw)
 {
-    int sum_pulses[20], nLshifts[20];
+    int32_t *sum_pulses = sw->sum_pulses, *nLshifts = sw->nLshifts;
     int RateLevelIndex = rd_icdf(rd, &T_silk_rate_levels_iCDF[(signalType >> 1) * 9], 8);
     int iter = frame_length >> 4;
     if (iter * 16 < frame_length) iter++;
@@ -717,7 +733,7 @@ DNI void silk_decode_pulses(RangeDec *rd, int16_t *pulses, int signalType, int q
         }
     }
     for (int i = 0; i < iter; i++) {
-        if (sum_pulses[i] > 0) silk_shell_decoder(&pulses[i * 16], rd, sum_pulses[i]);
+        if (sum_pulses[i] > 0) silk_shell_decoder(&pulses[i * 16], rd, sum_pulses[i], sw->shell);
         else for (int k = 0; k < 16; k++) pulses[i * 16 + k] = 0;
     }
     for (int i = 0; i < iter; i++) {
@@ -736,7 +752,7 @@ DNI void silk_decode_pulses(RangeDec *rd, int16_t *pulses, int signalType, int q
         }
     }
     // signs
-    uint8_t icdf[2];
+    uint8_t *icdf = sw->sign_icdf;
     icdf[1] = 0;
     const uint8_t *icdf_ptr = &T_silk_sign_iCDF[7 * (quantOffsetType + (signalType << 1))];
     int len = (frame_length + 8) >> 4;
@@ -811,21 +827,21 @@ DNI void silk_gains_dequant(int32_t *gain_Q16, const int8_t *ind, int32_t *prev_
     }
 }
 
-DNI void silk_decode_parameters(SilkChan *c, SilkCtrl *ctrl, int condCoding)
+DNI void silk_decode_parameters(SilkChan *c, SilkCtrl *ctrl, int condCoding, SilkWork *sw)
 {
-    int16_t pNLSF_Q15[16], pNLSF0_Q15[16];
+    int16_t *pNLSF_Q15 = sw->pNLSF_Q15, *pNLSF0_Q15 = sw->pNLSF0_Q15;
     SilkIndices *ix = &c->indices;
     silk_gains_dequant(ctrl->Gains_Q16, ix->GainsIndices, &c->LastGainIndex, condCoding == CODE_COND,
                        c->nb_subfr);
     NlsfCB cb = silk_nlsf_cb(c->LPC_order);
-    silk_nlsf_decode(pNLSF_Q15, ix->NLSFIndices, cb);
-    silk_nlsf2a(ctrl->PredCoef_Q12[1], pNLSF_Q15, c->LPC_order);
+    silk_nlsf_decode(pNLSF_Q15, ix->NLSFIndices, cb, sw);
+    silk_nlsf2a(ctrl->PredCoef_Q12[1], pNLSF_Q15, c->LPC_order, sw);
     if (c->first_frame_after_reset == 1) ix->NLSFInterpCoef_Q2 = 4;
     if (ix->NLSFInterpCoef_Q2 < 4) {
         for (int i = 0; i < c->LPC_order; i++)
             pNLSF0_Q15[i] = (int16_t)(c->prevNLSF_Q15[i] +
                 ((ix->NLSFInterpCoef_Q2 * (pNLSF_Q15[i] - c->prevNLSF_Q15[i])) >> 2));
-        silk_nlsf2a(ctrl->PredCoef_Q12[0], pNLSF0_Q15, c->LPC_order);
+        silk_nlsf2a(ctrl->PredCoef_Q12[0], pNLSF0_Q15, c->LPC_order, sw);
     } else {
         for (int i = 0; i < c->LPC_order; i++) ctrl->PredCoef_Q12[0][i] = ctrl->PredCoef_Q12[1][i];
     }
@@ -954,13 +970,26 @@ DNI void silk_decode_core(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *xq, con
         } else {
             pres = pexc;
         }
-        // LPC synthesis: order-10/16 recursion per sample
+        // LPC synthesis: order-10/16 recursion per sample.  The prediction is
+        // order/2 plus one truncated product per tap, summed with wrap-around
+        // adds, so the sum may be taken in any order: the taps on samples
+        // older than the newest one are summed while the newest sample is
+        // still being computed, and only tap 0 stays on the recursion's path.
         const int order = c->LPC_order;
-        for (int i = 0; i < c->subfr_length; i++) {
-            int32_t p = order >> 1;
+        int32_t pold = order >> 1;     // order/2 + taps 1.. on the current window
 #pragma unroll
-            for (int j = 0; j < 16; j++)
-                if (j < order) p = s_smlawb(p, win[15 - j], A_Q12[j]);
+        for (int j = 1; j < 16; j++)
+            if (j < order) pold = wadd(pold, s_smulwb(win[15 - j], A_Q12[j]));
+        for (int i = 0; i < c->subfr_length; i++) {
+            int32_t p = wadd(pold, s_smulwb(win[15], A_Q12[0]));
+            // taps 1.. of the next sample read win[16 - j]: known already
+            int32_t pa = order >> 1, pb = 0;
+#pragma unroll
+            for (int j = 1; j < 16; j += 2) {
+                if (j < order) pa = wadd(pa, s_smulwb(win[16 - j], A_Q12[j]));
+                if (j + 1 < order) pb = wadd(pb, s_smulwb(win[15 - j], A_Q12[j + 1]));
+            }
+            pold = wadd(pa, pb);
             int32_t v = s_add_sat32(pres[i], s_lshift_sat32(p, 4));
 #pragma unroll
             for (int t = 0; t < 15; t++) win[t] = win[t + 1];
@@ -1017,9 +1046,8 @@ DNI void silk_plc_update(SilkChan *c, const SilkCtrl *ctrl)
 
 DNI void silk_plc_conceal(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *frame, SilkScratch *w)
 {
-    const int16_t HARM_ATT_Q15[2] = {32440, 31130};
-    const int16_t RAND_ATT_V_Q15[2] = {31130, 26214};
-    const int16_t RAND_ATT_UV_Q15[2] = {32440, 29491};
+    // HARM_ATT_Q15 {32440, 31130}, RAND_ATT_V_Q15 {31130, 26214}, RAND_ATT_UV_Q15
+    // {32440, 29491} of silk/PLC.c, indexed by min(1, lossCnt)
     SilkPLC *p = &c->sPLC;
     int32_t *sLTP_Q14 = w->sLTP_Q15;
     int16_t *sLTP = w->sLTP;
@@ -1045,9 +1073,10 @@ DNI void silk_plc_conceal(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *frame, 
         rand_ptr = &c->exc_Q14[imax(0, p->nb_subfr * p->subfr_length - 128)];
     int16_t *B_Q14 = p->LTPCoef_Q14;
     int16_t rand_scale_Q14 = p->randScale_Q14;
-    int32_t harm_Gain_Q15 = HARM_ATT_Q15[imin(1, c->lossCnt)];
-    int32_t rand_Gain_Q15 = c->prevSignalType == SIG_VOICED ? RAND_ATT_V_Q15[imin(1, c->lossCnt)]
-                                                            : RAND_ATT_UV_Q15[imin(1, c->lossCnt)];
+    const int first_loss = c->lossCnt == 0;
+    int32_t harm_Gain_Q15 = first_loss ? 32440 : 31130;
+    int32_t rand_Gain_Q15 = c->prevSignalType == SIG_VOICED ? (first_loss ? 31130 : 26214)
+                                                            : (first_loss ? 32440 : 29491);
     silk_bwexpander(p->prevLPC_Q12, c->LPC_order, 64881);   // SILK_FIX_CONST(0.99, 16)
     int16_t A_Q12[16];
     for (int i = 0; i < c->LPC_order; i++) A_Q12[i] = p->prevLPC_Q12[i];
@@ -1058,7 +1087,7 @@ DNI void silk_plc_conceal(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *frame, 
             rand_scale_Q14 = rand_scale_Q14 > 3277 ? rand_scale_Q14 : 3277;
             rand_scale_Q14 = (int16_t)(s_smulbb(rand_scale_Q14, p->prevLTP_scale_Q14) >> 14);
         } else {
-            int32_t invGain_Q30 = silk_lpc_inv_pred_gain(p->prevLPC_Q12, c->LPC_order);
+            int32_t invGain_Q30 = silk_lpc_inv_pred_gain(p->prevLPC_Q12, c->LPC_order, w->sw.A);
             int32_t down = min32((1 << 30) >> 3, invGain_Q30);
             down = max32((1 << 30) >> 8, down);
             down = shl32(down, 3);
@@ -1206,7 +1235,7 @@ DNI void silk_cng(SilkChan *c, const SilkCtrl *ctrl, int16_t *frame, int length,
         }
         g->rand_seed = seed;
         int16_t A_Q12[16];
-        silk_nlsf2a(A_Q12, g->CNG_smth_NLSF_Q15, c->LPC_order);
+        silk_nlsf2a(A_Q12, g->CNG_smth_NLSF_Q15, c->LPC_order, &w->sw);
         for (int i = 0; i < 16; i++) sig[i] = g->CNG_synth_state[i];
         for (int i = 0; i < length; i++) {
             int32_t pr = c->LPC_order >> 1;
@@ -1233,13 +1262,14 @@ DNI void silk_decode_frame(Lanes L, SilkChan *c, RangeDec *rd, int16_t *pOut, in
     if (lostFlag == LOSS_NONE || (lostFlag == LOSS_LBRR && c->LBRR_flags[c->nFramesDecoded] == 1)) {
         int16_t *pulses = w->pulses;
         PHASE_BEGIN(t_ix);
-        silk_decode_indices(c, rd, c->nFramesDecoded, lostFlag, condCoding);
+        silk_decode_indices(c, rd, c->nFramesDecoded, lostFlag, condCoding, &w->sw);
         PHASE_END(PH_SILK_INDICES, t_ix, L.id);
         PHASE_BEGIN(t_pu);
-        silk_decode_pulses(rd, pulses, c->indices.signalType, c->indices.quantOffsetType, c->frame_length);
+        silk_decode_pulses(rd, pulses, c->indices.signalType, c->indices.quantOffsetType, c->frame_length,
+                           &w->sw);
         PHASE_END(PH_SILK_PULSES, t_pu, L.id);
         PHASE_BEGIN(t_pa);
-        silk_decode_parameters(c, ctrl, condCoding);
+        silk_decode_parameters(c, ctrl, condCoding, &w->sw);
         PHASE_END(PH_SILK_PARAMS, t_pa, L.id);
         PHASE_BEGIN(t_co);
         silk_decode_core(L, c, ctrl, pOut, pulses, w);
@@ -1375,9 +1405,9 @@ DNI int silk_decode(Lanes L, SilkDec *dec, SilkDecControl *ctl, int lostFlag, in
                                 decode_only_middle = rd_icdf(rd, T_silk_stereo_only_code_mid_iCDF, 8);
                         }
                         int cond = (i > 0 && cs[n].LBRR_flags[i - 1]) ? CODE_COND : CODE_INDEP;
-                        silk_decode_indices(&cs[n], rd, i, 1, cond);
+                        silk_decode_indices(&cs[n], rd, i, 1, cond, &w->sw);
                         silk_decode_pulses(rd, w->lbrr_pulses, cs[n].indices.signalType,
-                                           cs[n].indices.quantOffsetType, cs[n].frame_length);
+                                           cs[n].indices.quantOffsetType, cs[n].frame_length, &w->sw);
                     }
                 }
             }

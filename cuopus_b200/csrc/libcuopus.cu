@@ -851,6 +851,48 @@ extern "C" int cuopus_autotune(const cuopus_batch *b, const int32_t *widths, int
     return RC_OK;
 }
 
+extern "C" int cuopus_autotune_occupancy(const cuopus_batch *b, const int32_t *groups_per_sm, int n, int reps,
+                                         void *cuda_stream, int32_t *best_max_groups, float *times_ms,
+                                         char *errbuf, size_t errcap)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    Err err(errbuf, errcap);
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    if (!b || !groups_per_sm || n <= 0 || !best_max_groups) return err.set(RC_ARG, "autotune: bad arguments");
+    int rc = refuse_capture(st, err);
+    if (rc) return rc;
+    if ((rc = ensure_occupancy(err))) return rc;
+    if (reps < 1) reps = 1;
+    float best = -1.f;
+    for (int i = 0; i < n; i++) {
+        cuopus_batch c = *b;
+        c.max_groups = groups_per_sm[i] > 0 ? groups_per_sm[i] * G.sm_count : 0;
+        std::vector<float> t;
+        bool ok = groups_per_sm[i] >= 0;
+        for (int r = 0; r < reps && ok; r++) {
+            float ms = 0.f;
+            Err e2(nullptr, 0);
+            int rc2 = decode_batch(&c, st, &ms, e2);
+            if (rc2 == RC_CUDA) return err.set(rc2, "autotune: %s", e2.buf);
+            ok = rc2 == RC_OK;
+            t.push_back(ms);
+        }
+        float med = -1.f;
+        if (ok) {
+            std::sort(t.begin(), t.end());
+            med = t[t.size() / 2];
+            if (best < 0.f || med < best) {
+                best = med;
+                *best_max_groups = c.max_groups;
+            }
+        }
+        if (times_ms) times_ms[i] = med;
+    }
+    CK(cudaStreamSynchronize(st));
+    if (best < 0.f) return err.set(RC_ARG, "autotune: no candidate could be launched");
+    return RC_OK;
+}
+
 extern "C" int cuopus_resample48to16(const int16_t *in_dev, int64_t avail, int64_t n_out, float *out_dev,
                                      void *cuda_stream, char *errbuf, size_t errcap)
 {

@@ -89,6 +89,10 @@ def _load():
     lib.cuopus_autotune.argtypes = [ctypes.POINTER(Batch), c_p, ctypes.c_int, c_p, ctypes.c_int, ctypes.c_int, c_p,
                                     ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), c_p,
                                     ctypes.c_char_p, ctypes.c_size_t]
+    lib.cuopus_autotune_occupancy.restype = ctypes.c_int
+    lib.cuopus_autotune_occupancy.argtypes = [ctypes.POINTER(Batch), c_p, ctypes.c_int, ctypes.c_int, c_p,
+                                              ctypes.POINTER(ctypes.c_int32), c_p, ctypes.c_char_p,
+                                              ctypes.c_size_t]
     lib.cuopus_last_stats.restype = ctypes.c_int
     lib.cuopus_last_stats.argtypes = [c_p]
     lib.cuopus_resample48to16.restype = ctypes.c_int
@@ -320,6 +324,22 @@ def autotune(batch: Batch, widths=(4, 8, 16, 32), blocks=(32, 64, 128), reps=1, 
     table = {(int(w[i]), int(b[j])): (float(t[i * len(b) + j]) if t[i * len(b) + j] >= 0 else None)
              for i in range(len(w)) for j in range(len(b))}
     return bw.value, bb.value, table
+
+
+def autotune_occupancy(batch: Batch, groups_per_sm=(0, 7, 6, 5, 4), reps=1, stream=None):
+    """Extension: time the batch (its width and block kept) at every count of
+    decoder groups per SM (0 = all resident groups); returns
+    (best max_groups for cuopus_batch, {groups_per_sm: median ms or None})."""
+    import numpy as np
+    lib = _load()
+    g = np.ascontiguousarray(np.array(groups_per_sm, np.int32))
+    t = np.zeros(len(g), np.float32)
+    best = ctypes.c_int32(0)
+    err = ctypes.create_string_buffer(_ERRCAP)
+    _check(lib.cuopus_autotune_occupancy(ctypes.byref(batch), g.ctypes.data, len(g), int(reps),
+                                         ctypes.c_void_p(stream or 0), ctypes.byref(best), t.ctypes.data, err,
+                                         _ERRCAP), err)
+    return best.value, {int(g[i]): (float(t[i]) if t[i] >= 0 else None) for i in range(len(g))}
 
 
 class Stats(ctypes.Structure):

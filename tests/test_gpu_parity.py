@@ -228,3 +228,38 @@ def test_inband_fec_matches_libopus(cuda, fec):
             assert np.array_equal(g["nsamp"], ref["nsamp"][i]) and np.array_equal(g["rng"], ref["rng"][i])
             assert np.array_equal(g["pcm"], ref["pcm"][i]), "stream %d chain %d" % (s, i)
         k += len(chs[s])
+
+
+def test_autotuners_pick_a_launch_and_keep_the_bits(cuda):
+    """cuopus_autotune (width x block) and cuopus_autotune_occupancy (decoder
+    groups per SM) time real candidates, and the launch they pick decodes the
+    same samples as libopus."""
+    import torch
+    from cuopus_b200 import cuopus_native as cn
+    from gpu_util import device_batch, run_device_batch
+    rng = np.random.default_rng(91)
+    streams = [corpus.make_stream(dict(kind="mixed", seed=9100 + s, seconds=float(rng.uniform(0.5, 4)),
+                                       channels=1 + s % 2)) for s in range(40)]
+    idx = [ogg_port.demux(d) for d in streams]
+    pk = [ix["packets"] for ix in idx]
+    nch = [ix["channels"] for ix in idx]
+    b, T, meta = device_batch(pk, [[(0, len(p))] for p in pk], nch)
+    b.schedule, b.graph = 1, 1
+    order = np.arange(meta["n"], dtype=np.uint32)[::-1].copy()
+    b.order = order.ctypes.data
+    st = torch.cuda.current_stream().cuda_stream
+    w, blk, table = cn.autotune(b, widths=(8, 32), blocks=(64, 128), reps=1, stream=st)
+    assert (w, blk) in table and table[(w, blk)] == min(v for v in table.values() if v is not None)
+    b.width, b.block = w, blk
+    mg, occ = cn.autotune_occupancy(b, groups_per_sm=(0, 6, 4), reps=1, stream=st)
+    assert set(occ) == {0, 6, 4} and all(v is not None and v > 0 for v in occ.values())
+    assert mg in (0, 6 * torch.cuda.get_device_properties(0).multi_processor_count,
+                  4 * torch.cuda.get_device_properties(0).multi_processor_count)
+    b.max_groups = mg
+    res = run_device_batch(b, meta, width=w, schedule=1, order=order, block=blk, graph=1)
+    out = T["out"].cpu().numpy()
+    for s in range(len(pk)):
+        ref = ref_decode.decode_chains(pk[s], [(0, len(pk[s]))], nch[s])
+        assert int(res[s, 0]) == 0 and int(res[s, 1]) == int(ref["samples"][0])
+        o = int(meta["out_off"][s])
+        assert np.array_equal(out[o:o + int(meta["keep"][s]) * nch[s]], ref["pcm"][0])
