@@ -584,6 +584,7 @@ def main():
         os.environ["CUOPUS_SEG_S"] = str(seg)
         os.environ["CUOPUS_MAX_BATCH"] = str(10 ** 8)
         os.environ["CUOPUS_STRIDE"] = str(info["width"])
+        os.environ["CUOPUS_DEMUX_THREADS"] = str(threads)     # demux the files on every host core
 
         f16k = args.workload == "long7200"
         if f16k:     # the drop-in f16k path: float32 16 kHz output, read back
@@ -631,7 +632,8 @@ def main():
                "h2d_bytes_per_step": int(sum(map(len, files))),
                "d2h_bytes_per_step": int(4 * sum(n16)) if f16k else int(2 * sum(caps)),
                "ms_per_step": e2e_s * 1e3, "api": "cuopus_decode_f16k_multi (float32 16 kHz)" if f16k else
-               "cuopus_decode_i16_multi (int16 48 kHz)"}
+               "cuopus_decode_i16_multi (int16 48 kHz)", "demux_threads": threads,
+               "last_call": {k: (round(v, 2) if isinstance(v, float) else v) for k, v in cn.last_stats().items()}}
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_budget > 0:

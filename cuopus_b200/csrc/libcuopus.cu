@@ -22,10 +22,12 @@
 #include <time.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/cuopus.h"
@@ -141,6 +143,19 @@ int default_width()
     int p = 1;
     while (p * 2 <= w && p < 32) p *= 2;
     return p;
+}
+
+// Decoder warps per SM of the library's own launches (CUOPUS_WARPS_PER_SM,
+// default 5): fewer than the GPU holds (8 at 128-thread blocks), because the
+// decoder waits on instruction fetch when more of its warps share an SM, so
+// each chain decodes faster and the longest chains finish sooner (the
+// occupancy autotuner measured 5 per SM best on the mixed batch).  Returns
+// the cuopus_batch.max_groups value for `width` lanes per chain.
+int default_max_groups(int width)
+{
+    int wps = env_i("CUOPUS_WARPS_PER_SM", 5);
+    if (G.sm_count <= 0 || wps <= 0) return 0;
+    return wps * G.sm_count * (32 / width);
 }
 
 int refuse_capture(cudaStream_t st, Err &err)
@@ -390,20 +405,66 @@ struct Plan {
     uint64_t out_elems = 0;
 };
 
+// One file's demux and chain table, with each chain's decode capacity.
+struct FilePlan {
+    cuo_host::Demux d;
+    cuo_host::Chains c;
+    std::vector<uint64_t> capn;
+    std::string e;
+    bool ok = false;
+};
+
+void plan_one(const uint8_t *ogg, size_t n, double seg_s, double preroll_ms, bool require_mono, FilePlan &F)
+{
+    F.ok = cuo_host::demux_and_chain(ogg, n, seg_s, preroll_ms, require_mono, F.d, &F.c, F.e);
+    if (!F.ok) return;
+    F.capn.resize(F.c.size());
+    for (uint32_t i = 0; i < F.c.size(); i++) {
+        uint64_t capn = 0;
+        for (uint32_t k = 0; k < F.c.npkts[i]; k++) {
+            uint32_t p = F.c.first[i] + k;
+            capn += (uint64_t)cuo_host::toc_samples48(F.d.blob.data() + F.d.off[p], F.d.len[p]);
+        }
+        F.capn[i] = capn;
+    }
+}
+
+// Demux every file and merge the tables.  The files are demuxed on
+// CUOPUS_DEMUX_THREADS host threads (default 1: the calling thread only, as
+// the reference's library, which starts no threads); errors are reported for
+// the lowest-numbered failing file, whatever the thread count.
 int plan_files(const uint8_t *const *oggs, const size_t *ns, int nfiles, bool require_mono, Plan &P, Err &err)
 {
     double seg_s = env_f("CUOPUS_SEG_S", 1.0);
     double preroll_ms = env_f("CUOPUS_PREROLL_MS", 250.0);
-    for (int f = 0; f < nfiles; f++) {
+    for (int f = 0; f < nfiles; f++)
         if (!oggs || !ns || !oggs[f] || !ns[f]) return err.set(RC_ARG, "file %d: empty input", f);
-        cuo_host::Demux d;
-        cuo_host::Chains c;
-        std::string e;
-        if (!cuo_host::demux_and_chain(oggs[f], ns[f], seg_s, preroll_ms, require_mono, d, &c, e))
-        {
-            if (nfiles > 1) return err.set(RC_SOFT, "file %d: %s", f, e.c_str());
-            return err.set(RC_SOFT, "%s", e.c_str());
+    std::vector<FilePlan> F((size_t)std::max(nfiles, 0));
+    int nthreads = std::min(env_i("CUOPUS_DEMUX_THREADS", 1), std::max(nfiles, 1));
+    if (nthreads > 64) nthreads = 64;
+    std::atomic<int> next(0);
+    auto work = [&]() {
+        for (int f; (f = next.fetch_add(1)) < nfiles;)
+            plan_one(oggs[f], ns[f], seg_s, preroll_ms, require_mono, F[f]);
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthreads; t++) {
+        try {
+            pool.emplace_back(work);
+        } catch (...) {
+            break;   // fewer threads; the calling thread does the rest
         }
+    }
+    work();
+    for (auto &t : pool) t.join();
+    for (int f = 0; f < nfiles; f++) {
+        FilePlan &Fp = F[f];
+        if (!Fp.ok) {
+            if (nfiles > 1) return err.set(RC_SOFT, "file %d: %s", f, Fp.e.c_str());
+            return err.set(RC_SOFT, "%s", Fp.e.c_str());
+        }
+        const cuo_host::Demux &d = Fp.d;
+        const cuo_host::Chains &c = Fp.c;
         uint64_t pkt_base = P.len.size(), data_base = P.blob.size();
         P.blob.insert(P.blob.end(), d.blob.begin(), d.blob.end());
         for (uint32_t k = 0; k < d.n_packets(); k++) {
@@ -413,11 +474,7 @@ int plan_files(const uint8_t *const *oggs, const size_t *ns, int nfiles, bool re
         uint64_t fkeep = 0;
         P.file_out0.push_back(P.out_elems);
         for (uint32_t i = 0; i < c.size(); i++) {
-            uint64_t capn = 0;
-            for (uint32_t k = 0; k < c.npkts[i]; k++) {
-                uint32_t p = c.first[i] + k;
-                capn += (uint64_t)cuo_host::toc_samples48(d.blob.data() + d.off[p], d.len[p]);
-            }
+            uint64_t capn = Fp.capn[i];
             if (capn < (uint64_t)c.trim[i] + c.keep[i])
                 return err.set(RC_SOFT, "chain %u capacity %llu < trim %u + keep %u", i,
                                (unsigned long long)capn, c.trim[i], c.keep[i]);
@@ -496,6 +553,8 @@ int run_plan(const Plan &P, cudaStream_t st, Err &err)
     b.res = (uint32_t *)G.res.p;
     b.nchains = (int32_t)nch;
     b.width = default_width();
+    if ((rc = ensure_occupancy(err))) return rc;
+    b.max_groups = default_max_groups(b.width);
     // longest chains first through the device queue: packets are the proxy
     std::vector<uint32_t> order(nch);
     std::iota(order.begin(), order.end(), 0u);

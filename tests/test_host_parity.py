@@ -344,3 +344,32 @@ def test_host_decoder_inband_fec_matches_libopus(hc, seed, channels):
         assert stop == int(ref["status"][i]), i
         assert np.array_equal(ns, ref["nsamp"][i]) and np.array_equal(rg, ref["rng"][i]), i
         assert np.array_equal(pcm, ref["pcm"][i]), i
+
+
+def test_parallel_demux_reports_like_the_sequential_one(cn, monkeypatch):
+    """CUOPUS_DEMUX_THREADS: the file entry points demux on several host
+    threads and still report the lowest-numbered bad file, with the same code
+    and message as on the calling thread alone (no GPU needed: the demux comes
+    first)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("checks the pre-GPU part of the call on a machine without a GPU")
+    lib = cn.lib()
+    good = [_stream(n) for n in ("mixed_stereo_a", "mixed_mono_b", "plain_b", "long_hybrid")]
+    bad = b"OggS" + b"\x07" * 200
+    files = [good[0], good[1], bad, good[2], bad, good[3]]
+    n = len(files)
+    ba = (ctypes.c_char_p * n)(*files)
+    la = (ctypes.c_size_t * n)(*[len(f) for f in files])
+    outs = (ctypes.c_void_p * n)()
+    caps = (ctypes.c_size_t * n)()
+    lens = (ctypes.c_int64 * n)()
+    chans = (ctypes.c_int32 * n)()
+    seen = set()
+    for threads in ("1", "4", "16"):
+        monkeypatch.setenv("CUOPUS_DEMUX_THREADS", threads)
+        err = ctypes.create_string_buffer(512)
+        rc = lib.cuopus_decode_i16_multi(ba, la, n, outs, caps, lens, chans, None, err, 512)
+        assert rc == 1
+        seen.add(err.value)
+    assert len(seen) == 1 and next(iter(seen)).startswith(b"file 2:")
