@@ -2079,6 +2079,35 @@ DNI void celt_decode_lost(Lanes L, CeltDec *st, int N, int LM, CeltScratch *w)
 
 // ------------------------------------------------------------------ frame decode
 
+// The band energies of the first frame after a loss that is not intra coded
+// (celt/celt_decoder.c, in celt_decode_with_ec_dred before unquant_coarse_energy):
+// each energy may rise at most as the previous two frames did, less a safety
+// margin.  Its own function, so the code of the lossless path stays small.
+DNI void energy_after_loss(CeltDec *st, int start, int end, int LM)
+{
+    int16_t *oldBandE = st->oldBandE, *oldLogE = st->oldLogE, *oldLogE2 = st->oldLogE2;
+    for (int c = 0; c < 2; c++) {
+        int16_t safety = 0;
+        int missing = imin(10, st->loss_duration >> LM);
+        if (LM == 0) safety = 1536;
+        else if (LM == 1) safety = 512;
+        for (int i = start; i < end; i++) {
+            int16_t *e0 = &oldBandE[c * CELT_NB + i];
+            int16_t e1 = oldLogE[c * CELT_NB + i], e2 = oldLogE2[c * CELT_NB + i];
+            if (*e0 < (e1 > e2 ? e1 : e2)) {
+                int32_t E0 = *e0, E1 = e1, E2 = e2;
+                int32_t slope = max32(E1 - E0, (E2 - E0) >> 1);
+                E0 -= max32(0, (1 + missing) * slope);
+                *e0 = (int16_t)max32(-20480, E0);   // -QCONST16(20.f, DB_SHIFT)
+            } else {
+                int16_t m = *e0 < e1 ? *e0 : e1;
+                *e0 = m < e2 ? m : e2;
+            }
+            *e0 = (int16_t)(*e0 - safety);
+        }
+    }
+}
+
 // celt/celt_decoder.c celt_decode_with_ec_dred (downsample 1, no deep PLC).
 // data == 0 or len <= 1 runs the concealment.  Returns samples or < 0.
 DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t *pcm, int frame_size,
@@ -2113,9 +2142,10 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
     }
     int16_t *oldBandE = st->oldBandE, *oldLogE = st->oldLogE, *oldLogE2 = st->oldLogE2,
             *backgroundLogE = st->backgroundLogE;
-    if (C == 1)
-        for (int i = 0; i < CELT_NB; i++)
-            oldBandE[i] = oldBandE[i] > oldBandE[CELT_NB + i] ? oldBandE[i] : oldBandE[CELT_NB + i];
+    if (C == 1) {
+        LFOR(L, i, 0, CELT_NB) oldBandE[i] = oldBandE[i] > oldBandE[CELT_NB + i] ? oldBandE[i] : oldBandE[CELT_NB + i];
+        lsync(L);
+    }
     int32_t total_bits = len * 8;
     int32_t tell = rd_tell(dec);
     int silence;
@@ -2147,28 +2177,7 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
     }
     int shortBlocks = isTransient ? M : 0;
     int intra_ener = tell + 3 <= total_bits ? rd_bit_logp(dec, 3) : 0;
-    if (!intra_ener && st->loss_duration != 0) {
-        for (int c = 0; c < 2; c++) {
-            int16_t safety = 0;
-            int missing = imin(10, st->loss_duration >> LM);
-            if (LM == 0) safety = 1536;
-            else if (LM == 1) safety = 512;
-            for (int i = start; i < end; i++) {
-                int16_t *e0 = &oldBandE[c * CELT_NB + i];
-                int16_t e1 = oldLogE[c * CELT_NB + i], e2 = oldLogE2[c * CELT_NB + i];
-                if (*e0 < (e1 > e2 ? e1 : e2)) {
-                    int32_t E0 = *e0, E1 = e1, E2 = e2;
-                    int32_t slope = max32(E1 - E0, (E2 - E0) >> 1);
-                    E0 -= max32(0, (1 + missing) * slope);
-                    *e0 = (int16_t)max32(-20480, E0);   // -QCONST16(20.f, DB_SHIFT)
-                } else {
-                    int16_t m = *e0 < e1 ? *e0 : e1;
-                    *e0 = m < e2 ? m : e2;
-                }
-                *e0 = (int16_t)(*e0 - safety);
-            }
-        }
-    }
+    if (!intra_ener && st->loss_duration != 0) energy_after_loss(st, start, end, LM);
     PHASE_BEGIN(t_ce);
     unquant_coarse_energy(start, end, oldBandE, intra_ener, dec, C, LM);
     PHASE_END(PH_CELT_COARSE, t_ce, L.id);
@@ -2255,29 +2264,29 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
         st->postfilter_gain_old = st->postfilter_gain;
         st->postfilter_tapset_old = st->postfilter_tapset;
     }
-    if (C == 1)
-        for (int i = 0; i < CELT_NB; i++) oldBandE[CELT_NB + i] = oldBandE[i];
-    if (!isTransient) {
-        for (int i = 0; i < 2 * CELT_NB; i++) oldLogE2[i] = oldLogE[i];
-        for (int i = 0; i < 2 * CELT_NB; i++) oldLogE[i] = oldBandE[i];
-    } else {
-        for (int i = 0; i < 2 * CELT_NB; i++) oldLogE[i] = oldLogE[i] < oldBandE[i] ? oldLogE[i] : oldBandE[i];
+    // energy history: every band of both channels on its own, so lanes split them
+    if (C == 1) {
+        LFOR(L, i, 0, CELT_NB) oldBandE[CELT_NB + i] = oldBandE[i];
+        lsync(L);
     }
     int32_t mbi = imin(160, st->loss_duration + M) * 1;   // QCONST16(0.001f, DB_SHIFT) == 1
-    for (int i = 0; i < 2 * CELT_NB; i++) {
-        int32_t v = backgroundLogE[i] + mbi;
-        backgroundLogE[i] = (int16_t)(v < oldBandE[i] ? v : oldBandE[i]);
-    }
-    for (int c = 0; c < 2; c++) {
-        for (int i = 0; i < start; i++) {
-            oldBandE[c * CELT_NB + i] = 0;
-            oldLogE[c * CELT_NB + i] = oldLogE2[c * CELT_NB + i] = -28672;
+    LFOR(L, j, 0, 2 * CELT_NB) {
+        int16_t e = oldBandE[j];
+        if (!isTransient) {
+            oldLogE2[j] = oldLogE[j];
+            oldLogE[j] = e;
+        } else {
+            oldLogE[j] = oldLogE[j] < e ? oldLogE[j] : e;
         }
-        for (int i = end; i < CELT_NB; i++) {
-            oldBandE[c * CELT_NB + i] = 0;
-            oldLogE[c * CELT_NB + i] = oldLogE2[c * CELT_NB + i] = -28672;
+        int32_t v = backgroundLogE[j] + mbi;
+        backgroundLogE[j] = (int16_t)(v < e ? v : e);
+        int i = j < CELT_NB ? j : j - CELT_NB;
+        if (i < start || i >= end) {
+            oldBandE[j] = 0;
+            oldLogE[j] = oldLogE2[j] = -28672;
         }
     }
+    lsync(L);
     st->rng = dec->rng;
     PHASE_BEGIN(t_de);
     deemphasis(L, out_syn[0], out_syn[1], pcm, N, CC, st->preemph_memD, accum);

@@ -143,7 +143,8 @@ struct KeepWindow {
     int16_t *out;
     int channels;
     uint64_t pos, trim, keep;
-    MFN void operator()(const int16_t *frame, int n)
+    // a call, not inlined: frames are emitted from several places
+    MNI void operator()(const int16_t *frame, int n)
     {
         uint64_t lo = pos > trim ? pos : trim;
         uint64_t hi = pos + (uint64_t)n < trim + keep ? pos + (uint64_t)n : trim + keep;

@@ -26,12 +26,14 @@
 #define DFN static __device__ __forceinline__
 #define MFN __device__ __forceinline__
 #define DNI static __device__ __noinline__
+#define MNI __device__ __noinline__
 #define TABC(type, decl) static __constant__ type decl
 #define TABG(type, decl) static __device__ const type decl
 #else
 #define DFN static inline
 #define MFN inline
 #define DNI static
+#define MNI
 #define TABC(type, decl) static const type decl
 #define TABG(type, decl) static const type decl
 #endif

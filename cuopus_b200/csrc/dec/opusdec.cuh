@@ -392,7 +392,7 @@ DFN int packet_nb_samples(const uint8_t *data, int32_t len)
 // Concealment of n samples per channel (src/opus_decoder.c:715-729, the
 // len == 0 branch of opus_decode_native), emitted frame by frame.
 template <class Emit>
-DFN int conceal_samples(Lanes L, OpusDec *st, int n, int16_t *frame_buf, OpusScratch *w, Emit &emit)
+DNI int conceal_samples(Lanes L, OpusDec *st, int n, int16_t *frame_buf, OpusScratch *w, Emit &emit)
 {
     int pcm_count = 0;
     do {

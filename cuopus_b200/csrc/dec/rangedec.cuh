@@ -62,14 +62,14 @@ DNI void rd_init(RangeDec *d, const uint8_t *buf, uint32_t storage)
     rd_normalize(d);
 }
 
-DFN unsigned rd_decode(RangeDec *d, unsigned ft)
+DNI unsigned rd_decode(RangeDec *d, unsigned ft)
 {
     d->ext = d->rng / ft;
     unsigned s = d->val / d->ext;
     return ft - (s + 1 < ft ? s + 1 : ft);
 }
 
-DFN unsigned rd_decode_bin(RangeDec *d, unsigned bits)
+DNI unsigned rd_decode_bin(RangeDec *d, unsigned bits)
 {
     d->ext = d->rng >> bits;
     unsigned s = d->val / d->ext;
@@ -77,7 +77,7 @@ DFN unsigned rd_decode_bin(RangeDec *d, unsigned bits)
     return t - (s + 1u < t ? s + 1u : t);
 }
 
-DFN void rd_update(RangeDec *d, unsigned fl, unsigned fh, unsigned ft)
+DNI void rd_update(RangeDec *d, unsigned fl, unsigned fh, unsigned ft)
 {
     uint32_t s = d->ext * (ft - fh);
     d->val -= s;
@@ -85,7 +85,7 @@ DFN void rd_update(RangeDec *d, unsigned fl, unsigned fh, unsigned ft)
     rd_normalize(d);
 }
 
-DFN int rd_bit_logp(RangeDec *d, unsigned logp)
+DNI int rd_bit_logp(RangeDec *d, unsigned logp)
 {
     uint32_t r = d->rng, v = d->val;
     uint32_t s = r >> logp;

@@ -132,7 +132,7 @@ struct SilkWork {
     uint8_t pred_Q8[16];
     int16_t pNLSF_Q15[16], pNLSF0_Q15[16];                // silk_decode_parameters
     int32_t sum_pulses[20], nLshifts[20];                 // silk_decode_pulses
-    int16_t shell[14];                                    // shell split tree: p3[2], p2[4], p1[8]
+    int16_t shell[14];                                    // shell split tree walk: stack
     uint8_t sign_icdf[2];
 };
 
@@ -681,38 +681,36 @@ DNI void silk_decode_indices(SilkChan *c, RangeDec *rd, int FrameIndex, int deco
     ix->Seed = (int8_t)rd_icdf(rd, T_silk_uniform4_iCDF, 8);
 }
 
-DFN void silk_shell_split(int16_t *p1, int16_t *p2, RangeDec *rd, int p, const uint8_t *table)
-{
-    if (p > 0) {
-        p1[0] = (int16_t)rd_icdf(rd, &table[T_silk_shell_code_table_offsets[p]], 8);
-        p2[0] = (int16_t)(p - p1[0]);
-    } else {
-        p1[0] = 0;
-        p2[0] = 0;
-    }
-}
-
-// silk/shell_coder.c silk_shell_decoder: binary split tree over 16 pulses
+// silk/shell_coder.c silk_shell_decoder: a binary split tree over 16 pulses.
+// libopus unrolls the tree; here one loop walks it depth first, left half
+// before right half, which reads the splits in the same order.  A node at
+// level L (3 = the root) holds the pulse count of 2^(L+1) positions; its split
+// gives the left child's count from the level-L table, the right child gets
+// the rest.  `tree` is scratch for the walk's stack (8 entries).
 DNI void silk_shell_decoder(int16_t *p0, RangeDec *rd, int pulses4, int16_t *tree)
 {
-    int16_t *p3 = tree, *p2 = tree + 2, *p1 = tree + 6;
-    const uint8_t *t0 = T_silk_shell_code_table0, *t1 = T_silk_shell_code_table1,
-                  *t2 = T_silk_shell_code_table2, *t3 = T_silk_shell_code_table3;
-    silk_shell_split(&p3[0], &p3[1], rd, pulses4, t3);
-    silk_shell_split(&p2[0], &p2[1], rd, p3[0], t2);
-    silk_shell_split(&p1[0], &p1[1], rd, p2[0], t1);
-    silk_shell_split(&p0[0], &p0[1], rd, p1[0], t0);
-    silk_shell_split(&p0[2], &p0[3], rd, p1[1], t0);
-    silk_shell_split(&p1[2], &p1[3], rd, p2[1], t1);
-    silk_shell_split(&p0[4], &p0[5], rd, p1[2], t0);
-    silk_shell_split(&p0[6], &p0[7], rd, p1[3], t0);
-    silk_shell_split(&p2[2], &p2[3], rd, p3[1], t2);
-    silk_shell_split(&p1[4], &p1[5], rd, p2[2], t1);
-    silk_shell_split(&p0[8], &p0[9], rd, p1[4], t0);
-    silk_shell_split(&p0[10], &p0[11], rd, p1[5], t0);
-    silk_shell_split(&p1[6], &p1[7], rd, p2[3], t1);
-    silk_shell_split(&p0[12], &p0[13], rd, p1[6], t0);
-    silk_shell_split(&p0[14], &p0[15], rd, p1[7], t0);
+    int sp = 0;
+    tree[sp++] = (int16_t)(pulses4 | 3 << 5);                 // count | level << 5 | first position << 8
+    while (sp > 0) {
+        int node = tree[--sp];
+        int p = node & 31, lvl = (node >> 5) & 3, pos = node >> 8;
+        int left = 0;
+        if (p > 0) {
+            const uint8_t *t = lvl == 3 ? T_silk_shell_code_table3
+                             : lvl == 2 ? T_silk_shell_code_table2
+                             : lvl == 1 ? T_silk_shell_code_table1 : T_silk_shell_code_table0;
+            left = rd_icdf(rd, &t[T_silk_shell_code_table_offsets[p]], 8);
+        }
+        int right = p - left;
+        if (lvl == 0) {
+            p0[pos] = (int16_t)left;
+            p0[pos + 1] = (int16_t)right;
+        } else {
+            int half = 1 << lvl;                                  // positions under each child
+            tree[sp++] = (int16_t)(right | (lvl - 1) << 5 | (pos + half) << 8);
+            tree[sp++] = (int16_t)(left | (lvl - 1) << 5 | pos << 8);
+        }
+    }
 }
 
 // silk/decode_pulses.c + code_signs.c silk_decode_signs
@@ -1187,6 +1185,45 @@ DNI void silk_plc_glue_frames(SilkChan *c, int16_t *frame, int length)
 }
 
 // silk/CNG.c
+// The comfort-noise generation of silk_CNG (only after a lost frame): its own
+// function, so the code of the per-frame update stays small.
+DNI void silk_cng_generate(SilkChan *c, int16_t *frame, int length, SilkScratch *w)
+{
+    SilkCNG *g = &c->sCNG;
+    int32_t *sig = w->CNG_sig_Q14;
+    int32_t gain_Q16 = s_smulww(c->sPLC.randScale_Q14, c->sPLC.prevGain_Q16[1]);
+    if (gain_Q16 >= (1 << 21) || g->CNG_smth_Gain_Q16 > (1 << 23)) {
+        gain_Q16 = s_smultt(gain_Q16, gain_Q16);
+        gain_Q16 = wsub(s_smultt(g->CNG_smth_Gain_Q16, g->CNG_smth_Gain_Q16), shl32(gain_Q16, 5));
+        gain_Q16 = shl32(s_sqrt_approx(gain_Q16), 16);
+    } else {
+        gain_Q16 = s_smulww(gain_Q16, gain_Q16);
+        gain_Q16 = wsub(s_smulww(g->CNG_smth_Gain_Q16, g->CNG_smth_Gain_Q16), shl32(gain_Q16, 5));
+        gain_Q16 = shl32(s_sqrt_approx(gain_Q16), 8);
+    }
+    int32_t gain_Q10 = gain_Q16 >> 6;
+    // silk_CNG_exc
+    int exc_mask = 255;
+    while (exc_mask > length) exc_mask >>= 1;
+    int32_t seed = g->rand_seed;
+    for (int i = 0; i < length; i++) {
+        seed = s_rand(seed);
+        sig[16 + i] = g->CNG_exc_buf_Q14[(seed >> 24) & exc_mask];
+    }
+    g->rand_seed = seed;
+    int16_t A_Q12[16];
+    silk_nlsf2a(A_Q12, g->CNG_smth_NLSF_Q15, c->LPC_order, &w->sw);
+    for (int i = 0; i < 16; i++) sig[i] = g->CNG_synth_state[i];
+    for (int i = 0; i < length; i++) {
+        int32_t pr = c->LPC_order >> 1;
+        for (int j = 0; j < c->LPC_order; j++) pr = s_smlawb(pr, sig[16 + i - j - 1], A_Q12[j]);
+        sig[16 + i] = s_add_sat32(sig[16 + i], s_lshift_sat32(pr, 4));
+        frame[i] = (int16_t)s_sat16((int32_t)frame[i] +
+            s_sat16(s_rshift_round(s_smulww(sig[16 + i], gain_Q10), 8)));
+    }
+    for (int i = 0; i < 16; i++) g->CNG_synth_state[i] = sig[length + i];
+}
+
 DNI void silk_cng(SilkChan *c, const SilkCtrl *ctrl, int16_t *frame, int length, SilkScratch *w)
 {
     SilkCNG *g = &c->sCNG;
@@ -1212,42 +1249,9 @@ DNI void silk_cng(SilkChan *c, const SilkCtrl *ctrl, int16_t *frame, int length,
                 g->CNG_smth_Gain_Q16 = ctrl->Gains_Q16[i];
         }
     }
-    if (c->lossCnt) {
-        int32_t *sig = w->CNG_sig_Q14;
-        int32_t gain_Q16 = s_smulww(c->sPLC.randScale_Q14, c->sPLC.prevGain_Q16[1]);
-        if (gain_Q16 >= (1 << 21) || g->CNG_smth_Gain_Q16 > (1 << 23)) {
-            gain_Q16 = s_smultt(gain_Q16, gain_Q16);
-            gain_Q16 = wsub(s_smultt(g->CNG_smth_Gain_Q16, g->CNG_smth_Gain_Q16), shl32(gain_Q16, 5));
-            gain_Q16 = shl32(s_sqrt_approx(gain_Q16), 16);
-        } else {
-            gain_Q16 = s_smulww(gain_Q16, gain_Q16);
-            gain_Q16 = wsub(s_smulww(g->CNG_smth_Gain_Q16, g->CNG_smth_Gain_Q16), shl32(gain_Q16, 5));
-            gain_Q16 = shl32(s_sqrt_approx(gain_Q16), 8);
-        }
-        int32_t gain_Q10 = gain_Q16 >> 6;
-        // silk_CNG_exc
-        int exc_mask = 255;
-        while (exc_mask > length) exc_mask >>= 1;
-        int32_t seed = g->rand_seed;
-        for (int i = 0; i < length; i++) {
-            seed = s_rand(seed);
-            sig[16 + i] = g->CNG_exc_buf_Q14[(seed >> 24) & exc_mask];
-        }
-        g->rand_seed = seed;
-        int16_t A_Q12[16];
-        silk_nlsf2a(A_Q12, g->CNG_smth_NLSF_Q15, c->LPC_order, &w->sw);
-        for (int i = 0; i < 16; i++) sig[i] = g->CNG_synth_state[i];
-        for (int i = 0; i < length; i++) {
-            int32_t pr = c->LPC_order >> 1;
-            for (int j = 0; j < c->LPC_order; j++) pr = s_smlawb(pr, sig[16 + i - j - 1], A_Q12[j]);
-            sig[16 + i] = s_add_sat32(sig[16 + i], s_lshift_sat32(pr, 4));
-            frame[i] = (int16_t)s_sat16((int32_t)frame[i] +
-                s_sat16(s_rshift_round(s_smulww(sig[16 + i], gain_Q10), 8)));
-        }
-        for (int i = 0; i < 16; i++) g->CNG_synth_state[i] = sig[length + i];
-    } else {
+    if (c->lossCnt) silk_cng_generate(c, frame, length, w);
+    else
         for (int i = 0; i < c->LPC_order; i++) g->CNG_synth_state[i] = 0;
-    }
 }
 
 // ------------------------------------------------------------------ frame
@@ -1339,6 +1343,30 @@ DNI void silk_stereo_ms_to_lr(Lanes L, SilkStereo *st, int16_t *x1, int16_t *x2,
 
 // silk/dec_API.c silk_Decode (API rate 48 kHz, no deep PLC).  Returns nonzero
 // on an invalid configuration.
+// Regular decoding reads past the packet's LBRR (in-band FEC) frames: their
+// indices and pulses are decoded and dropped (silk/dec_API.c).  Returns the
+// mid-only flag as the last LBRR frame left it.
+DNI int silk_skip_lbrr(SilkChan *cs, int nChannelsInternal, RangeDec *rd, int32_t *MS_pred_Q13,
+                       int decode_only_middle, SilkScratch *w)
+{
+    for (int i = 0; i < cs[0].nFramesPerPacket; i++) {
+        for (int n = 0; n < nChannelsInternal; n++) {
+            if (cs[n].LBRR_flags[i]) {
+                if (nChannelsInternal == 2 && n == 0) {
+                    silk_stereo_decode_pred(rd, MS_pred_Q13);
+                    if (cs[1].LBRR_flags[i] == 0)
+                        decode_only_middle = rd_icdf(rd, T_silk_stereo_only_code_mid_iCDF, 8);
+                }
+                int cond = (i > 0 && cs[n].LBRR_flags[i - 1]) ? CODE_COND : CODE_INDEP;
+                silk_decode_indices(&cs[n], rd, i, 1, cond, &w->sw);
+                silk_decode_pulses(rd, w->lbrr_pulses, cs[n].indices.signalType, cs[n].indices.quantOffsetType,
+                                   cs[n].frame_length, &w->sw);
+            }
+        }
+    }
+    return decode_only_middle;
+}
+
 DNI int silk_decode(Lanes L, SilkDec *dec, SilkDecControl *ctl, int lostFlag, int newPacketFlag,
                     RangeDec *rd, int16_t *samplesOut, int32_t *nSamplesOut, SilkScratch *w)
 {
@@ -1394,24 +1422,8 @@ DNI int silk_decode(Lanes L, SilkDec *dec, SilkDecControl *ctl, int lostFlag, in
                 }
             }
         }
-        if (lostFlag == LOSS_NONE) {
-            // regular decoding: skip all LBRR data
-            for (int i = 0; i < cs[0].nFramesPerPacket; i++) {
-                for (int n = 0; n < ctl->nChannelsInternal; n++) {
-                    if (cs[n].LBRR_flags[i]) {
-                        if (ctl->nChannelsInternal == 2 && n == 0) {
-                            silk_stereo_decode_pred(rd, MS_pred_Q13);
-                            if (cs[1].LBRR_flags[i] == 0)
-                                decode_only_middle = rd_icdf(rd, T_silk_stereo_only_code_mid_iCDF, 8);
-                        }
-                        int cond = (i > 0 && cs[n].LBRR_flags[i - 1]) ? CODE_COND : CODE_INDEP;
-                        silk_decode_indices(&cs[n], rd, i, 1, cond, &w->sw);
-                        silk_decode_pulses(rd, w->lbrr_pulses, cs[n].indices.signalType,
-                                           cs[n].indices.quantOffsetType, cs[n].frame_length, &w->sw);
-                    }
-                }
-            }
-        }
+        if (lostFlag == LOSS_NONE && (cs[0].LBRR_flag || (ctl->nChannelsInternal == 2 && cs[1].LBRR_flag)))
+            decode_only_middle = silk_skip_lbrr(cs, ctl->nChannelsInternal, rd, MS_pred_Q13, decode_only_middle, w);
     }
     if (ctl->nChannelsInternal == 2) {
         if (lostFlag == LOSS_NONE ||
