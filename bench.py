@@ -11,7 +11,7 @@ encoder (oracle/corpus.py), generated before anything is timed.
 A step is one decode of the whole batch.
   value      scheduled form: persistent grid pulling chains from a device work
              queue, longest first by the learned cost model, replayed as a CUDA
-             graph, width x block and decoder groups per SM picked by the
+             graph, width x block and decoder warps per SM picked by the
              autotuner; packets and chain
              tables already in HBM; CUDA-event time on the launching stream
   plain      the plain one-launch form on the same batch: one warp per chain,
@@ -302,7 +302,7 @@ def schedule_batch(cn, db, stream, args):
         info["order"] = "learned (MLP 16-64-64-1)"
         info["cost_model"] = {"train_s": round(time.time() - t0, 2), "loss_first": float(losses[0]),
                               "loss_last": float(losses[-1]), "r2_log_cycles": round(float(r2), 4)}
-    # autotune width x block on the scheduled form, then the decoder groups per SM
+    # autotune width x block on the scheduled form, then the decoder warps per SM
     width, block, max_groups = args.width, args.block, 0
     sched = {"queue": 1, "static": 0, "plain": 2}[args.schedule]
     if not args.no_tune:
@@ -312,9 +312,9 @@ def schedule_batch(cn, db, stream, args):
         info["autotune"] = {"%dx%d" % k: (round(v, 1) if v else None) for k, v in table.items()}
         if sched != 2:
             b = db.batch(width, sched, order if sched == 1 else None, block, 1)
-            max_groups, occ = cn.autotune_occupancy(b, groups_per_sm=(0, 7, 6, 5, 4), reps=2,
+            max_groups, occ = cn.autotune_occupancy(b, warps_per_sm=(0, 7, 6, 5, 4), reps=2,
                                                     stream=stream.cuda_stream)
-            info["autotune_groups_per_sm"] = {str(k): (round(v, 1) if v else None) for k, v in occ.items()}
+            info["autotune_warps_per_sm"] = {str(k): (round(v, 1) if v else None) for k, v in occ.items()}
     b = db.batch(width, sched, order if sched == 1 else None, block, 1 if sched != 2 else 0)
     b.max_groups = max_groups
     info.update(width=width, block=block, max_groups=max_groups)

@@ -910,14 +910,14 @@ extern "C" int cuopus_autotune(const cuopus_batch *b, const int32_t *widths, int
     return RC_OK;
 }
 
-extern "C" int cuopus_autotune_occupancy(const cuopus_batch *b, const int32_t *groups_per_sm, int n, int reps,
+extern "C" int cuopus_autotune_occupancy(const cuopus_batch *b, const int32_t *warps_per_sm, int n, int reps,
                                          void *cuda_stream, int32_t *best_max_groups, float *times_ms,
                                          char *errbuf, size_t errcap)
 {
     std::lock_guard<std::mutex> lk(g_mu);
     Err err(errbuf, errcap);
     cudaStream_t st = (cudaStream_t)cuda_stream;
-    if (!b || !groups_per_sm || n <= 0 || !best_max_groups) return err.set(RC_ARG, "autotune: bad arguments");
+    if (!b || !warps_per_sm || n <= 0 || !best_max_groups) return err.set(RC_ARG, "autotune: bad arguments");
     int rc = refuse_capture(st, err);
     if (rc) return rc;
     if ((rc = ensure_occupancy(err))) return rc;
@@ -925,9 +925,10 @@ extern "C" int cuopus_autotune_occupancy(const cuopus_batch *b, const int32_t *g
     float best = -1.f;
     for (int i = 0; i < n; i++) {
         cuopus_batch c = *b;
-        c.max_groups = groups_per_sm[i] > 0 ? groups_per_sm[i] * G.sm_count : 0;
+        int width = c.width > 0 ? c.width : 32;
+        c.max_groups = warps_per_sm[i] > 0 ? warps_per_sm[i] * G.sm_count * (32 / width) : 0;
         std::vector<float> t;
-        bool ok = groups_per_sm[i] >= 0;
+        bool ok = warps_per_sm[i] >= 0 && width >= 1 && width <= 32;
         for (int r = 0; r < reps && ok; r++) {
             float ms = 0.f;
             Err e2(nullptr, 0);

@@ -326,13 +326,13 @@ def autotune(batch: Batch, widths=(4, 8, 16, 32), blocks=(32, 64, 128), reps=1, 
     return bw.value, bb.value, table
 
 
-def autotune_occupancy(batch: Batch, groups_per_sm=(0, 7, 6, 5, 4), reps=1, stream=None):
+def autotune_occupancy(batch: Batch, warps_per_sm=(0, 7, 6, 5, 4), reps=1, stream=None):
     """Extension: time the batch (its width and block kept) at every count of
-    decoder groups per SM (0 = all resident groups); returns
-    (best max_groups for cuopus_batch, {groups_per_sm: median ms or None})."""
+    decoder warps per SM (0 = all resident groups); returns
+    (best max_groups for cuopus_batch, {warps_per_sm: median ms or None})."""
     import numpy as np
     lib = _load()
-    g = np.ascontiguousarray(np.array(groups_per_sm, np.int32))
+    g = np.ascontiguousarray(np.array(warps_per_sm, np.int32))
     t = np.zeros(len(g), np.float32)
     best = ctypes.c_int32(0)
     err = ctypes.create_string_buffer(_ERRCAP)

@@ -163,14 +163,15 @@ int cuopus_autotune(const cuopus_batch *b, const int32_t *widths, int nwidths, c
 
 /* Extension: occupancy autotuner of the persistent launch.  Decodes the batch
  * (width, block, schedule, order and graph of *b kept) `reps` times for every
- * count of decoder groups per SM in groups_per_sm[0..n) (0 = every resident
+ * count of decoder warps per SM in warps_per_sm[0..n) (0 = every resident
  * group) and returns in *best_max_groups the cuopus_batch.max_groups value
- * (groups per SM x SMs, 0 for all) with the lowest median kernel time.
- * Fewer resident groups than the GPU holds can decode faster: the decoder is
+ * (warps per SM x SMs x lane groups per warp, 0 for all) with the lowest
+ * median kernel time.
+ * Fewer resident warps than the GPU holds can decode faster: the decoder is
  * one large body of code, and with fewer warps per SM at different places in
  * it each warp waits less for instructions, so a chain decodes faster and the
  * longest chains finish sooner.  times_ms (may be NULL) receives n medians. */
-int cuopus_autotune_occupancy(const cuopus_batch *b, const int32_t *groups_per_sm, int n, int reps,
+int cuopus_autotune_occupancy(const cuopus_batch *b, const int32_t *warps_per_sm, int n, int reps,
                               void *cuda_stream, int32_t *best_max_groups, float *times_ms, char *errbuf,
                               size_t errcap);
 

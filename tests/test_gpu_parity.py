@@ -232,7 +232,7 @@ def test_inband_fec_matches_libopus(cuda, fec):
 
 def test_autotuners_pick_a_launch_and_keep_the_bits(cuda):
     """cuopus_autotune (width x block) and cuopus_autotune_occupancy (decoder
-    groups per SM) time real candidates, and the launch they pick decodes the
+    warps per SM) time real candidates, and the launch they pick decodes the
     same samples as libopus."""
     import torch
     from cuopus_b200 import cuopus_native as cn
@@ -251,10 +251,10 @@ def test_autotuners_pick_a_launch_and_keep_the_bits(cuda):
     w, blk, table = cn.autotune(b, widths=(8, 32), blocks=(64, 128), reps=1, stream=st)
     assert (w, blk) in table and table[(w, blk)] == min(v for v in table.values() if v is not None)
     b.width, b.block = w, blk
-    mg, occ = cn.autotune_occupancy(b, groups_per_sm=(0, 6, 4), reps=1, stream=st)
+    mg, occ = cn.autotune_occupancy(b, warps_per_sm=(0, 6, 4), reps=1, stream=st)
     assert set(occ) == {0, 6, 4} and all(v is not None and v > 0 for v in occ.values())
-    assert mg in (0, 6 * torch.cuda.get_device_properties(0).multi_processor_count,
-                  4 * torch.cuda.get_device_properties(0).multi_processor_count)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    assert mg in (0, 6 * sms * (32 // w), 4 * sms * (32 // w))
     b.max_groups = mg
     res = run_device_batch(b, meta, width=w, schedule=1, order=order, block=blk, graph=1)
     out = T["out"].cpu().numpy()
