@@ -105,6 +105,36 @@ DFN int32_t lsum(const Lanes &L, int32_t v)
     return v;
 }
 
+// Exclusive prefix composition of affine maps x -> a*x + b (mod 2^32) over the
+// lanes of the group, lane 0's map first: on return (a, b) is the composition
+// of the maps of the lanes before this one, the identity on lane 0.  Modular
+// arithmetic is exact, so any grouping of the compositions gives the serial
+// result.
+DFN void lscan_affine(const Lanes &L, uint32_t &a, uint32_t &b)
+{
+#ifdef __CUDA_ARCH__
+    for (int off = 1; off < L.n; off <<= 1) {
+        uint32_t pa = __shfl_up_sync(L.mask, a, off, L.n), pb = __shfl_up_sync(L.mask, b, off, L.n);
+        if (L.id >= off) {   // this lane's span after the earlier one
+            b = a * pb + b;
+            a = a * pa;
+        }
+    }
+    uint32_t pa = __shfl_up_sync(L.mask, a, 1, L.n), pb = __shfl_up_sync(L.mask, b, 1, L.n);
+    if (L.id == 0) {
+        a = 1;
+        b = 0;
+    } else {
+        a = pa;
+        b = pb;
+    }
+#else
+    (void)L;
+    a = 1;
+    b = 0;
+#endif
+}
+
 // buf[i] = buf[i + shift] for i = 0 .. n-1 (the forward in-place copy that
 // drops the oldest `shift` samples of a history buffer), split across the
 // lanes.  Positions go in blocks of `shift`: block k reads only block k+1,

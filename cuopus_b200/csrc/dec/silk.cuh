@@ -207,22 +207,25 @@ DNI void silk_resampler_init48(SilkResampler *S, int32_t Fs_Hz_in)
 }
 
 // silk/resampler_private_up2_HQ.c: 2x up-sampling by two 3-stage all-pass chains
-DNI void silk_up2_hq(int32_t *S, int16_t *out, const int16_t *in, int32_t len)
+// The even and the odd outputs come from two all-pass cascades that share
+// only the input (states S[0..2] and S[3..5]), so two lanes run one cascade
+// each; a group of one lane runs them one after the other.
+DNI void silk_up2_hq(Lanes L, int32_t *S, int16_t *out, const int16_t *in, int32_t len)
 {
-    const int16_t *a0 = T_silk_resampler_up2_hq_0, *a1 = T_silk_resampler_up2_hq_1;
-    int32_t s0 = S[0], s1 = S[1], s2 = S[2], s3 = S[3], s4 = S[4], s5 = S[5];
-    for (int32_t k = 0; k < len; k++) {
-        int32_t in32 = shl32((int32_t)in[k], 10), Y, X, o1, o2;
-        Y = wsub(in32, s0); X = s_smulwb(Y, a0[0]); o1 = wadd(s0, X); s0 = wadd(in32, X);
-        Y = wsub(o1, s1); X = s_smulwb(Y, a0[1]); o2 = wadd(s1, X); s1 = wadd(o1, X);
-        Y = wsub(o2, s2); X = s_smlawb(Y, Y, a0[2]); o1 = wadd(s2, X); s2 = wadd(o2, X);
-        out[2 * k] = (int16_t)s_sat16(s_rshift_round(o1, 10));
-        Y = wsub(in32, s3); X = s_smulwb(Y, a1[0]); o1 = wadd(s3, X); s3 = wadd(in32, X);
-        Y = wsub(o1, s4); X = s_smulwb(Y, a1[1]); o2 = wadd(s4, X); s4 = wadd(o1, X);
-        Y = wsub(o2, s5); X = s_smlawb(Y, Y, a1[2]); o1 = wadd(s5, X); s5 = wadd(o2, X);
-        out[2 * k + 1] = (int16_t)s_sat16(s_rshift_round(o1, 10));
+    const int step = L.n > 1 ? 2 : 1;
+    for (int ph = L.n > 1 ? L.id : 0; ph < 2; ph += step) {
+        const int16_t *a = ph ? T_silk_resampler_up2_hq_1 : T_silk_resampler_up2_hq_0;
+        int32_t s0 = S[3 * ph], s1 = S[3 * ph + 1], s2 = S[3 * ph + 2];
+        for (int32_t k = 0; k < len; k++) {
+            int32_t in32 = shl32((int32_t)in[k], 10), Y, X, o1, o2;
+            Y = wsub(in32, s0); X = s_smulwb(Y, a[0]); o1 = wadd(s0, X); s0 = wadd(in32, X);
+            Y = wsub(o1, s1); X = s_smulwb(Y, a[1]); o2 = wadd(s1, X); s1 = wadd(o1, X);
+            Y = wsub(o2, s2); X = s_smlawb(Y, Y, a[2]); o1 = wadd(s2, X); s2 = wadd(o2, X);
+            out[2 * k + ph] = (int16_t)s_sat16(s_rshift_round(o1, 10));
+        }
+        S[3 * ph] = s0; S[3 * ph + 1] = s1; S[3 * ph + 2] = s2;
     }
-    S[0] = s0; S[1] = s1; S[2] = s2; S[3] = s3; S[4] = s4; S[5] = s5;
+    lsync(L);
 }
 
 // silk/resampler_private_IIR_FIR.c; the FIR interpolation is split over lanes
@@ -235,7 +238,7 @@ DNI int16_t *silk_iir_fir(Lanes L, SilkResampler *S, int16_t *out, const int16_t
     int32_t nIn = 0;
     while (1) {
         nIn = inLen < S->batchSize ? inLen : S->batchSize;
-        silk_up2_hq(S->sIIR, &buf[8], in, nIn);
+        silk_up2_hq(L, S->sIIR, &buf[8], in, nIn);
         lsync(L);
         int32_t max_index_Q16 = shl32(nIn, 17);
         int32_t nOut = (max_index_Q16 + inc - 1) / inc;
@@ -877,17 +880,33 @@ DNI void silk_decode_core(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *xq, con
     int32_t offset_Q10 = T_silk_Quantization_Offsets_Q10[(ix->signalType >> 1) * 2 + ix->quantOffsetType];
     int NLSF_interpolation_flag = ix->NLSFInterpCoef_Q2 < 4;
 
-    // excitation: the LCG sign flips make this a serial scan
-    int32_t rand_seed = ix->Seed;
-    for (int i = 0; i < c->frame_length; i++) {
-        rand_seed = s_rand(rand_seed);
-        int32_t e = shl32((int32_t)pulses[i], 14);
-        if (e > 0) e -= 80 << 4;
-        else if (e < 0) e += 80 << 4;
-        e += offset_Q10 << 4;
-        if (rand_seed < 0) e = -e;
-        c->exc_Q14[i] = e;
-        rand_seed = wadd(rand_seed, pulses[i]);
+    // excitation.  Sample i's sign comes from an LCG seed that then advances
+    // by the sample's pulse: t[i+1] = A (t[i] + p[i]) + B mod 2^32, an affine
+    // recurrence.  Each lane takes a contiguous run of samples, composes its
+    // run's maps, and a prefix composition over the lanes gives every run its
+    // first seed -- the serial seeds exactly (modular arithmetic).
+    {
+        const uint32_t A = 196314165u, B = 907633515u;   // silk_RAND
+        const int n = c->frame_length;
+        const int run = (n + L.n - 1) / L.n;
+        const int i0 = imin(n, L.id * run), i1 = imin(n, i0 + run);
+        uint32_t ma = 1, mb = 0;
+        for (int i = i0; i < i1; i++) {
+            mb = A * (mb + (uint32_t)(int32_t)pulses[i]) + B;
+            ma = A * ma;
+        }
+        lscan_affine(L, ma, mb);
+        uint32_t t = ma * (uint32_t)s_rand(ix->Seed) + mb;
+        for (int i = i0; i < i1; i++) {
+            int32_t e = shl32((int32_t)pulses[i], 14);
+            if (e > 0) e -= 80 << 4;
+            else if (e < 0) e += 80 << 4;
+            e += offset_Q10 << 4;
+            if ((int32_t)t < 0) e = -e;
+            c->exc_Q14[i] = e;
+            t = A * (t + (uint32_t)(int32_t)pulses[i]) + B;
+        }
+        lsync(L);
     }
     // LPC synthesis history: the last 16 outputs, in registers (win[15] newest)
     int32_t win[16];
@@ -1224,7 +1243,7 @@ DNI void silk_cng_generate(SilkChan *c, int16_t *frame, int length, SilkScratch 
     for (int i = 0; i < 16; i++) g->CNG_synth_state[i] = sig[length + i];
 }
 
-DNI void silk_cng(SilkChan *c, const SilkCtrl *ctrl, int16_t *frame, int length, SilkScratch *w)
+DNI void silk_cng(Lanes L, SilkChan *c, const SilkCtrl *ctrl, int16_t *frame, int length, SilkScratch *w)
 {
     SilkCNG *g = &c->sCNG;
     if (c->fs_kHz != g->fs_kHz) {
@@ -1239,10 +1258,16 @@ DNI void silk_cng(SilkChan *c, const SilkCtrl *ctrl, int16_t *frame, int length,
         int subfr = 0;
         for (int i = 0; i < c->nb_subfr; i++)
             if (ctrl->Gains_Q16[i] > max_Gain_Q16) { max_Gain_Q16 = ctrl->Gains_Q16[i]; subfr = i; }
-        for (int i = (c->nb_subfr - 1) * c->subfr_length - 1; i >= 0; i--)
-            g->CNG_exc_buf_Q14[c->subfr_length + i] = g->CNG_exc_buf_Q14[i];
-        for (int i = 0; i < c->subfr_length; i++)
-            g->CNG_exc_buf_Q14[i] = c->exc_Q14[subfr * c->subfr_length + i];
+        // the excitation history moves up by one subframe: blocks of one
+        // subframe from the top, each reading only what the block before it
+        // has already moved; lanes split a block
+        const int S = c->subfr_length;
+        for (int hi = (c->nb_subfr - 1) * S; hi > 0; hi -= S) {
+            LFOR(L, i, hi - S, hi) g->CNG_exc_buf_Q14[S + i] = g->CNG_exc_buf_Q14[i];
+            lsync(L);
+        }
+        LFOR(L, i, 0, S) g->CNG_exc_buf_Q14[i] = c->exc_Q14[subfr * S + i];
+        lsync(L);
         for (int i = 0; i < c->nb_subfr; i++) {
             g->CNG_smth_Gain_Q16 += s_smulwb(ctrl->Gains_Q16[i] - g->CNG_smth_Gain_Q16, 4634);
             if (s_smulww(g->CNG_smth_Gain_Q16, 46396) > ctrl->Gains_Q16[i])
@@ -1296,7 +1321,7 @@ DNI void silk_decode_frame(Lanes L, SilkChan *c, RangeDec *rd, int16_t *pOut, in
         lsync(L);
     }
     PHASE_BEGIN(t_cn);
-    silk_cng(c, ctrl, pOut, Lf, w);
+    silk_cng(L, c, ctrl, pOut, Lf, w);
     PHASE_END(PH_SILK_CNG, t_cn, L.id);
     silk_plc_glue_frames(c, pOut, Lf);
     c->lagPrev = ctrl->pitchL[c->nb_subfr - 1];
