@@ -74,7 +74,7 @@ DFN bool stage_wait(PacketStage &S, int b)
 
 // Start staging packet (src, n) into buffer b.  Returns false when the packet
 // is read in place instead (too long, staging off).
-DFN bool stage_issue(const Lanes &L, PacketStage &S, int b, const uint8_t *src, int n)
+DNI bool stage_issue(const Lanes &L, PacketStage &S, int b, const uint8_t *src, int n)
 {
     if (!S.ok || n <= 0 || n > STAGE_BUF - 32) return false;
     uintptr_t a = (uintptr_t)src;

@@ -404,6 +404,41 @@ DNI int conceal_samples(Lanes L, OpusDec *st, int n, int16_t *frame_buf, OpusScr
     return pcm_count;
 }
 
+// The decode_fec = 1 branch of opus_decode_native (src/opus_decoder.c:745-779)
+// for a parsed packet whose first frame is data[0 .. size0): conceal up to the
+// last frame, which comes from the packet's FEC data.  Its own function, so
+// the code of the lossless path stays small.
+template <class Emit>
+DNI int decode_fec(Lanes L, OpusDec *st, const uint8_t *data, int size0, int packet_mode, int packet_bandwidth,
+                   int packet_frame_size, int packet_stream_channels, int16_t *frame_buf, OpusScratch *w,
+                   Emit &emit)
+{
+    const int frame_size = MAX_PACKET_SAMPLES;
+    if (frame_size < packet_frame_size || packet_mode == MODE_CELT_ONLY || st->mode == MODE_CELT_ONLY) {
+        int ret = conceal_samples(L, st, frame_size, frame_buf, w, emit);
+        if (ret < 0) return ret;
+        st->last_packet_duration = ret;
+        return ret;
+    }
+    int duration_copy = st->last_packet_duration;
+    if (frame_size - packet_frame_size != 0) {
+        int ret = conceal_samples(L, st, frame_size - packet_frame_size, frame_buf, w, emit);
+        if (ret < 0) {
+            st->last_packet_duration = duration_copy;
+            return ret;
+        }
+    }
+    st->mode = packet_mode;
+    st->bandwidth = packet_bandwidth;
+    st->frame_size = packet_frame_size;
+    st->stream_channels = packet_stream_channels;
+    int ret = opus_frame<0>(L, st, data, size0, frame_buf, packet_frame_size, w, 1);
+    if (ret < 0) return ret;
+    emit(frame_buf, ret);
+    st->last_packet_duration = frame_size;
+    return frame_size;
+}
+
 // src/opus_decoder.c opus_decode_native (:670-811; not self-delimited,
 // frame_size = MAX_PACKET_SAMPLES).  `emit(frame_pcm, n)` receives each decoded
 // frame (n samples per channel, interleaved) so the caller can place it; the
@@ -432,31 +467,9 @@ DFN int opus_decode_packet(Lanes L, OpusDec *st, const uint8_t *data, int32_t le
     int count = packet_parse(data, len, size, &offset);
     if (count < 0) return count;
     data += offset;
-    if (fec) {
-        if (frame_size < packet_frame_size || packet_mode == MODE_CELT_ONLY || st->mode == MODE_CELT_ONLY) {
-            int ret = conceal_samples(L, st, frame_size, frame_buf, w, emit);
-            if (ret < 0) return ret;
-            st->last_packet_duration = ret;
-            return ret;
-        }
-        int duration_copy = st->last_packet_duration;
-        if (frame_size - packet_frame_size != 0) {
-            int ret = conceal_samples(L, st, frame_size - packet_frame_size, frame_buf, w, emit);
-            if (ret < 0) {
-                st->last_packet_duration = duration_copy;
-                return ret;
-            }
-        }
-        st->mode = packet_mode;
-        st->bandwidth = packet_bandwidth;
-        st->frame_size = packet_frame_size;
-        st->stream_channels = packet_stream_channels;
-        int ret = opus_frame<0>(L, st, data, size[0], frame_buf, packet_frame_size, w, 1);
-        if (ret < 0) return ret;
-        emit(frame_buf, ret);
-        st->last_packet_duration = frame_size;
-        return frame_size;
-    }
+    if (fec)
+        return decode_fec(L, st, data, size[0], packet_mode, packet_bandwidth, packet_frame_size,
+                          packet_stream_channels, frame_buf, w, emit);
     if (count * packet_frame_size > frame_size) return OPUS_BUFFER_TOO_SMALL;
     st->mode = packet_mode;
     st->bandwidth = packet_bandwidth;

@@ -145,15 +145,18 @@ int default_width()
     return p;
 }
 
-// Decoder warps per SM of the library's own launches (CUOPUS_WARPS_PER_SM,
-// default 5): fewer than the GPU holds (8 at 128-thread blocks), because the
-// decoder waits on instruction fetch when more of its warps share an SM, so
-// each chain decodes faster and the longest chains finish sooner (the
-// occupancy autotuner measured 5 per SM best on the mixed batch).  Returns
-// the cuopus_batch.max_groups value for `width` lanes per chain.
+// Decoder warps per SM of the library's own launches (CUOPUS_WARPS_PER_SM).
+// At 32 lanes per chain the default is 5, fewer than the GPU holds (8 at
+// 128-thread blocks): the decoder waits on instruction fetch when more of its
+// warps share an SM, so each chain decodes faster and the longest chains
+// finish sooner (the occupancy autotuner measured 5 per SM best on the mixed
+// batch).  At narrower widths a warp decodes several chains and the default
+// is every resident group (the 2 h file in 1 s chains at 8 lanes per chain
+// decoded in 151 ms with every group, 232 ms at 5 warps per SM).  Returns the
+// cuopus_batch.max_groups value for `width` lanes per chain (0 = all).
 int default_max_groups(int width)
 {
-    int wps = env_i("CUOPUS_WARPS_PER_SM", 5);
+    int wps = env_i("CUOPUS_WARPS_PER_SM", width == 32 ? 5 : 0);
     if (G.sm_count <= 0 || wps <= 0) return 0;
     return wps * G.sm_count * (32 / width);
 }
