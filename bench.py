@@ -317,7 +317,11 @@ def schedule_batch(cn, db, stream, args):
             info["autotune_warps_per_sm"] = {str(k): (round(v, 1) if v else None) for k, v in occ.items()}
     b = db.batch(width, sched, order if sched == 1 else None, block, 1 if sched != 2 else 0)
     b.max_groups = max_groups
-    info.update(width=width, block=block, max_groups=max_groups)
+    if not args.no_tune and sched == 1 and width == 32:
+        # tail scheduling: the longest chains alone on SMs of their own
+        light, tails = cn.autotune_tail(b, light=(0, 8, 16, 32), reps=2, stream=stream.cuda_stream)
+        info["autotune_light_sms"] = {str(k): round(v, 1) for k, v in tails.items()}
+    info.update(width=width, block=block, max_groups=max_groups, light_sms=b.light_sms)
     return b, info
 
 

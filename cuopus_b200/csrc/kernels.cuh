@@ -45,7 +45,17 @@ struct DecodeArgs {
     int stage;                  // packets staged in shared memory (STAGE_BYTES per group)
     int scalar;                 // one active lane per group (the reference kernel's slot layout)
     int fec;                    // in-band FEC for lost packets (decode_chain)
+    // Tail scheduling (queue schedule, light_sms > 0): the warps of SMs whose id
+    // is below light_sms keep only light_warps of themselves and take the
+    // first long_chains positions of the order first; every other SM keeps
+    // heavy_warps.  queue_head[0] counts the long positions, queue_head[1] the
+    // rest; sm_rank[smid] counts the warps that arrived on each SM.
+    unsigned *sm_rank;
+    int light_sms, light_warps, heavy_warps, long_chains;
 };
+
+// Number of SM ids sm_rank covers (%smid is masked to it).
+enum { SM_RANK_SLOTS = 256 };
 
 // Shared memory a block of `block` threads at `width` lanes per chain uses for
 // packet staging; 0 (no staging) when it would exceed 48 KB per block.
@@ -72,6 +82,24 @@ __device__ __forceinline__ unsigned long long globaltimer_ns()
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
+}
+
+// Next queue position under tail scheduling: light groups take the long
+// positions [0, long_chains) first, the others the rest; each takes from the
+// other part when its own is used up.  nchains when nothing is left.
+__device__ __forceinline__ unsigned queue_next(const DecodeArgs &a, int light)
+{
+    const unsigned K = (unsigned)a.long_chains, n = (unsigned)a.nchains;
+    if (light) {
+        unsigned v = atomicAdd(&a.queue_head[0], 1u);
+        if (v < K) return v;
+        v = K + atomicAdd(&a.queue_head[1], 1u);
+        return v < n ? v : n;
+    }
+    unsigned v = K + atomicAdd(&a.queue_head[1], 1u);
+    if (v < n) return v;
+    v = atomicAdd(&a.queue_head[0], 1u);
+    return v < K ? v : n;
 }
 
 // Resident 128-thread blocks per SM the register allocation is sized for.
@@ -103,11 +131,23 @@ __global__ void __launch_bounds__(128, CUO_MIN_BLOCKS) k_decode_chains(DecodeArg
         stage_init(L, S, s_stage + (size_t)(threadIdx.x / W) * STAGE_BYTES);
         stage = &S;
     }
+    int light = 0;
+    if (a.light_sms > 0) {   // tail scheduling: keep this warp or leave (whole warps, before any decoding)
+        unsigned smid, r = 0;
+        asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+        if (lane == 0) r = atomicAdd(&a.sm_rank[smid % SM_RANK_SLOTS], 1u);
+        r = __shfl_sync(0xffffffffu, r, 0);
+        light = smid < (unsigned)a.light_sms;
+        if ((int)r >= (light ? a.light_warps : a.heavy_warps)) {
+            if (stage) stage_drain(L, *stage);
+            return;
+        }
+    }
     for (int it = 0; it < a.nchains; it++) {
         int pos;
         if (a.use_queue) {
             unsigned v = 0;
-            if (L.id == 0) v = atomicAdd(a.queue_head, 1u);
+            if (L.id == 0) v = a.long_chains > 0 ? queue_next(a, light) : atomicAdd(a.queue_head, 1u);
             v = __shfl_sync(L.mask, v, sub * W);
             pos = (int)v;
         } else {

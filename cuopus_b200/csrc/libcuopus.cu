@@ -38,6 +38,9 @@ namespace {
 
 enum { RC_OK = 0, RC_SOFT = 1, RC_CUDA = 2, RC_ARG = 3 };
 const int BLOCK = 128;
+// work queue: two position counters (tail scheduling uses both) and the
+// per-SM warp counters of tail scheduling
+const size_t QUEUE_BYTES = (2 + cuo::SM_RANK_SLOTS) * sizeof(unsigned);
 const double SWR_TAIL_48K = 48;   // samples the CPU path never flushes (libcuopus.cu:195-199)
 
 struct Err {
@@ -293,7 +296,7 @@ int launch_graph(const cuo::DecodeArgs &a, int blocks, int block, cudaStream_t s
         }
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(G.cap_stream, cudaStreamCaptureModeThreadLocal));
-        cudaError_t e1 = a.use_queue ? cudaMemsetAsync(G.queue.p, 0, sizeof(unsigned), G.cap_stream) : cudaSuccess;
+        cudaError_t e1 = a.use_queue ? cudaMemsetAsync(G.queue.p, 0, QUEUE_BYTES, G.cap_stream) : cudaSuccess;
         cudaError_t e2 = cuo::decode_kernel_launch(a, blocks, block, G.cap_stream);
         cudaError_t e3 = cudaStreamEndCapture(G.cap_stream, &g);
         if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
@@ -333,21 +336,27 @@ int decode_batch(const cuopus_batch *b, cudaStream_t st, float *kernel_ms, Err &
     if (block != 32 && block != 64 && block != 96 && block != 128)
         return err.set(RC_ARG, "block %d is not 32, 64, 96 or 128 threads", block);
     if (block % width) return err.set(RC_ARG, "width %d does not divide block %d", width, block);
+    const bool tail = b->light_sms > 0;
+    if (tail && (b->schedule != 1 || b->scalar))
+        return err.set(RC_ARG, "tail scheduling (light_sms) needs the queue schedule and every lane");
+    if (b->light_sms < 0 || b->long_chains < 0) return err.set(RC_ARG, "light_sms / long_chains < 0");
     int rc = ensure_occupancy(err);
     if (rc) return rc;
     if ((rc = ensure_events(err))) return rc;
     // plain: one group per chain, the hardware block scheduler assigns them;
-    // static / queue: a persistent grid of the resident groups
+    // static / queue: a persistent grid of the resident groups (under tail
+    // scheduling all of them: the warps themselves decide which stay)
     long long groups = b->schedule == 2 ? (long long)b->nchains
                                         : std::min<long long>(b->nchains, resident_groups(block, width));
-    if (b->max_groups > 0) groups = std::min<long long>(groups, b->max_groups);
+    if (tail) groups = resident_groups(block, width);
+    else if (b->max_groups > 0) groups = std::min<long long>(groups, b->max_groups);
     int gpb = block / width;
     long long blocks_ll = (groups + gpb - 1) / gpb;
     if (blocks_ll > 0x7fffffffLL) return err.set(RC_ARG, "too many chains for one launch");
     int blocks = (int)blocks_ll;
     long long nslots = blocks_ll * gpb;
     if ((rc = gpu_grow(G.slots, (size_t)nslots * sizeof(cuo::ChainSlot), err))) return rc;
-    if ((rc = gpu_grow(G.queue, sizeof(unsigned), err))) return rc;
+    if ((rc = gpu_grow(G.queue, QUEUE_BYTES, err))) return rc;
     const uint32_t *order_dev = nullptr;
     if (b->schedule == 1 && b->order) {
         if ((rc = gpu_grow(G.order, 4ull * b->nchains, err))) return rc;
@@ -378,11 +387,19 @@ int decode_batch(const cuopus_batch *b, cudaStream_t st, float *kernel_ms, Err &
     a.use_queue = b->schedule == 1;
     a.scalar = b->scalar != 0;
     a.fec = b->fec != 0;
+    if (tail) {
+        int gpw = 32 / width;
+        a.sm_rank = (unsigned *)G.queue.p + 2;
+        a.light_sms = b->light_sms;
+        a.light_warps = 1;
+        a.heavy_warps = b->max_groups > 0 ? std::max(1, (int)(b->max_groups / ((long long)G.sm_count * gpw))) : 64;
+        a.long_chains = std::min(b->long_chains, b->nchains);
+    }
     CK(cudaEventRecord(G.ev0, st));
     if (b->graph) {
         if ((rc = launch_graph(a, blocks, block, st, err))) return rc;
     } else {
-        if (a.use_queue) CK(cudaMemsetAsync(G.queue.p, 0, sizeof(unsigned), st));
+        if (a.use_queue) CK(cudaMemsetAsync(G.queue.p, 0, QUEUE_BYTES, st));
         CK(cuo::decode_kernel_launch(a, blocks, block, st));
     }
     CK(cudaEventRecord(G.ev1, st));

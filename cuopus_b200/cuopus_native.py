@@ -51,7 +51,8 @@ class Batch(ctypes.Structure):
                 ("pkt_rng", ctypes.c_void_p), ("res", ctypes.c_void_p), ("nchains", ctypes.c_int32),
                 ("width", ctypes.c_int32), ("schedule", ctypes.c_int32), ("max_groups", ctypes.c_int32),
                 ("order", ctypes.c_void_p), ("block", ctypes.c_int32), ("graph", ctypes.c_int32),
-                ("scalar", ctypes.c_int32), ("fec", ctypes.c_int32)]
+                ("scalar", ctypes.c_int32), ("fec", ctypes.c_int32), ("light_sms", ctypes.c_int32),
+                ("long_chains", ctypes.c_int32)]
 
 
 _lib = None
@@ -340,6 +341,21 @@ def autotune_occupancy(batch: Batch, warps_per_sm=(0, 7, 6, 5, 4), reps=1, strea
                                          ctypes.c_void_p(stream or 0), ctypes.byref(best), t.ctypes.data, err,
                                          _ERRCAP), err)
     return best.value, {int(g[i]): (float(t[i]) if t[i] >= 0 else None) for i in range(len(g))}
+
+
+def autotune_tail(batch: Batch, light=(0, 8, 16, 32), reps=2, stream=None):
+    """Extension: time the batch (queue schedule, its order longest first) with
+    tail scheduling at every count of light SMs (the longest chains, one per
+    light SM, each alone on its SM; 0 = off); sets batch.light_sms /
+    long_chains to the fastest and returns (best count, {count: median ms})."""
+    import statistics
+    table = {}
+    for k in light:
+        batch.light_sms = batch.long_chains = int(k)
+        table[int(k)] = statistics.median(decode_batch(batch, stream) for _ in range(max(1, reps)))
+    best = min(table, key=table.get)
+    batch.light_sms = batch.long_chains = best
+    return best, table
 
 
 class Stats(ctypes.Structure):

@@ -129,6 +129,13 @@ typedef struct cuopus_batch {
                             5760 concealed samples as without FEC, the last frame's worth
                             rebuilt from the next packet's LBRR data.  0: the reference's
                             protocol (decode_fec = 0 for every packet). */
+    int32_t light_sms;   /* tail scheduling (queue schedule, not scalar; 0 = off): on the SMs
+                            with id < light_sms one decoder warp runs alone and takes the first
+                            long_chains positions of `order` first, so the longest chains of an
+                            uneven batch decode at the speed of an unshared SM; every other SM
+                            runs max_groups / SMs warps (all resident if max_groups is 0).  The
+                            launch grid is then every resident group. */
+    int32_t long_chains;
 } cuopus_batch;
 
 int cuopus_decode_batch(const cuopus_batch *b, void *cuda_stream, float *kernel_ms, char *errbuf, size_t errcap);

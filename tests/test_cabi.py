@@ -90,3 +90,19 @@ def test_stage_timer_build_exports_both_headers():
     assert lib.cuopus_phase_count() == len(cn.PHASE_NAMES)
     out = subprocess.run(["nm", "-D", "--defined-only", LIB], capture_output=True, text=True).stdout
     assert "cuopus_phase_read" not in out
+
+
+def test_tail_scheduling_arguments_are_checked():
+    """light_sms needs the queue schedule and every lane: other combinations
+    are refused with RC 3 before any device work."""
+    from cuopus_b200 import cuopus_native as cn
+    lib = cn.lib()
+    b = cn.Batch()
+    for f in ("data", "off", "len", "first", "npkts", "channels", "trim", "keep", "res"):
+        setattr(b, f, 16)   # never dereferenced: the call is refused first
+    b.nchains, b.width, b.block, b.light_sms, b.long_chains = 4, 32, 64, 2, 2
+    err = ctypes.create_string_buffer(256)
+    for schedule, scalar in ((2, 0), (0, 0), (1, 1)):
+        b.schedule, b.scalar = schedule, scalar
+        rc = lib.cuopus_decode_batch(ctypes.byref(b), None, None, err, 256)
+        assert rc == 3 and b"tail scheduling" in err.value

@@ -263,3 +263,30 @@ def test_autotuners_pick_a_launch_and_keep_the_bits(cuda):
         assert int(res[s, 0]) == 0 and int(res[s, 1]) == int(ref["samples"][0])
         o = int(meta["out_off"][s])
         assert np.array_equal(out[o:o + int(meta["keep"][s]) * nch[s]], ref["pcm"][0])
+
+
+def test_tail_scheduling_keeps_the_bits(cuda):
+    """Tail scheduling (cuopus_batch.light_sms): the longest chains run alone on
+    their own SMs, the rest share the others; every chain still decodes to
+    libopus's samples, whichever warp takes it."""
+    import torch
+    from gpu_util import device_batch, run_device_batch
+    rng = np.random.default_rng(93)
+    lens = [12.0, 9.0] + [float(rng.uniform(0.3, 3.0)) for _ in range(30)]
+    streams = [corpus.make_stream(dict(kind="mixed", seed=9300 + s, seconds=L, channels=1 + s % 2))
+               for s, L in enumerate(lens)]
+    idx = [ogg_port.demux(d) for d in streams]
+    pk = [ix["packets"] for ix in idx]
+    nch = [ix["channels"] for ix in idx]
+    b, T, meta = device_batch(pk, [[(0, len(p))] for p in pk], nch)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    order = np.argsort(-np.array([len(p) * c for p, c in zip(pk, nch)]), kind="stable").astype(np.uint32)
+    for light, mg in ((4, 5 * sms), (2, 0)):
+        b.light_sms, b.long_chains, b.max_groups = light, light, mg
+        res = run_device_batch(b, meta, width=32, schedule=1, order=order, block=64, graph=1)
+        out = T["out"].cpu().numpy()
+        for s in range(len(pk)):
+            ref = ref_decode.decode_chains(pk[s], [(0, len(pk[s]))], nch[s])
+            assert int(res[s, 0]) == 0 and int(res[s, 1]) == int(ref["samples"][0])
+            o = int(meta["out_off"][s])
+            assert np.array_equal(out[o:o + int(meta["keep"][s]) * nch[s]], ref["pcm"][0]), (light, s)
