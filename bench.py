@@ -303,7 +303,9 @@ def schedule_batch(cn, db, stream, args):
         info["cost_model"] = {"train_s": round(time.time() - t0, 2), "loss_first": float(losses[0]),
                               "loss_last": float(losses[-1]), "r2_log_cycles": round(float(r2), 4)}
     # autotune width x block on the scheduled form, then the decoder warps per SM
-    width, block, max_groups = args.width, args.block, 0
+    width, block = args.width, args.block
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    max_groups = args.warps_per_sm * sms * (32 // width) if args.warps_per_sm > 0 else 0
     sched = {"queue": 1, "static": 0, "plain": 2}[args.schedule]
     if not args.no_tune:
         b = db.batch(32, 1, order, 128, 1)
@@ -460,6 +462,7 @@ def main():
     ap.add_argument("--count", type=int, default=None, help="override the stream count (development)")
     ap.add_argument("--width", type=int, default=32, help="lanes per chain when not autotuned")
     ap.add_argument("--block", type=int, default=128, help="threads per block when not autotuned")
+    ap.add_argument("--warps-per-sm", type=int, default=0, help="decoder warps per SM when not autotuned (0 = all)")
     ap.add_argument("--schedule", default="queue", choices=["queue", "static", "plain"])
     ap.add_argument("--order", default="mlp", choices=["mlp", "packets"])
     ap.add_argument("--no-tune", action="store_true")
