@@ -948,26 +948,31 @@ DNI void exp_rotation_dec(int16_t *X, int len, int stride, int K, int spread)
 }
 
 // celt/vq.c renormalise_vector
-DNI void renormalise_vector(int16_t *X, int N, int16_t gain)
+// (the energy is a wrap-around sum, so the lanes' partial sums give the serial
+// value; every element is scaled on its own)
+DNI void renormalise_vector(Lanes L, int16_t *X, int N, int16_t gain)
 {
-    int32_t E = 1;
-    for (int i = 0; i < N; i++) E = c_mac16(E, X[i], X[i]);
+    int32_t E = 0;
+    LFOR(L, i, 0, N) E = c_mac16(E, X[i], X[i]);
+    E = wadd(lsum(L, E), 1);
     int k = c_ilog2(E) >> 1;
     int32_t t = c_vshr(E, 2 * (k - 7));
     int16_t g = (int16_t)c_mul16_p15(c_rsqrt_norm(t), gain);
-    for (int i = 0; i < N; i++) X[i] = (int16_t)c_pshr(c_mul16(g, X[i]), k + 1);
+    LFOR(L, i, 0, N) X[i] = (int16_t)c_pshr(c_mul16(g, X[i]), k + 1);
+    lsync(L);
 }
 
 // celt/vq.c alg_unquant
-DNI unsigned alg_unquant(int16_t *X, int N, int K, int spread, int B, RangeDec *dec, int16_t gain,
+DNI unsigned alg_unquant(Lanes L, int16_t *X, int N, int K, int spread, int B, RangeDec *dec, int16_t gain,
                          int32_t *iy)
 {
     int32_t Ryy = cwrsi(N, K, rd_uint(dec, pvq_v(N, K)), iy);
-    // normalise_residual
+    // normalise_residual (every element on its own)
     int k = c_ilog2(Ryy) >> 1;
     int32_t t = c_vshr(Ryy, 2 * (k - 7));
     int16_t g = (int16_t)c_mul16_p15(c_rsqrt_norm(t), gain);
-    for (int i = 0; i < N; i++) X[i] = (int16_t)c_pshr(c_mul16(g, iy[i]), k + 1);
+    LFOR(L, i, 0, N) X[i] = (int16_t)c_pshr(c_mul16(g, iy[i]), k + 1);
+    lsync(L);
     exp_rotation_dec(X, N, B, K, spread);
     // extract_collapse_mask
     if (B <= 1) return 1;
@@ -1041,6 +1046,7 @@ DNI void interleave_hadamard(int16_t *X, int N0, int stride, int hadamard, int16
 }
 
 struct BandCtx {
+    Lanes L;
     int i;
     int intensity;
     int spread;
@@ -1175,7 +1181,7 @@ DNI unsigned quant_partition_leaf(BandCtx *ctx, int16_t *X, int N, int b, int B,
     }
     if (q != 0) {
         int K = get_pulses(q);
-        cm = alg_unquant(X, N, K, ctx->spread, B, ctx->ec, gain, ctx->w->iy);
+        cm = alg_unquant(ctx->L, X, N, K, ctx->spread, B, ctx->ec, gain, ctx->w->iy);
     } else {
         unsigned cm_mask = (unsigned)(1UL << B) - 1;
         fill &= cm_mask;
@@ -1196,7 +1202,7 @@ DNI unsigned quant_partition_leaf(BandCtx *ctx, int16_t *X, int N, int b, int B,
                 }
                 cm = fill;
             }
-            renormalise_vector(X, N, gain);
+            renormalise_vector(ctx->L, X, N, gain);
         }
     }
     return cm;
@@ -1385,19 +1391,24 @@ DNI unsigned quant_band(BandCtx *ctx, int16_t *X, int N, int b, int B, int16_t *
     return cm;
 }
 
-DNI void stereo_merge(int16_t *X, int16_t *Y, int16_t mid, int N)
+// (the two dot products are wrap-around sums, so the lanes' partial sums give
+// the serial values; every element is mixed on its own)
+DNI void stereo_merge(Lanes L, int16_t *X, int16_t *Y, int16_t mid, int N)
 {
     int32_t xp = 0, side = 0;
-    for (int j = 0; j < N; j++) {
+    LFOR(L, j, 0, N) {
         xp = c_mac16(xp, Y[j], X[j]);
         side = c_mac16(side, Y[j], Y[j]);
     }
+    xp = lsum(L, xp);
+    side = lsum(L, side);
     xp = c_mul16_32_q15(mid, xp);
     int16_t mid2 = (int16_t)(mid >> 1);
     int32_t El = wsub(wadd(c_mul16(mid2, mid2), side), 2 * xp);
     int32_t Er = wadd(wadd(c_mul16(mid2, mid2), side), 2 * xp);
     if (Er < 161061 || El < 161061) {   // QCONST32(6e-4f, 28)
-        for (int j = 0; j < N; j++) Y[j] = X[j];
+        LFOR(L, j, 0, N) Y[j] = X[j];
+        lsync(L);
         return;
     }
     int kl = c_ilog2(El) >> 1, kr = c_ilog2(Er) >> 1;
@@ -1407,12 +1418,13 @@ DNI void stereo_merge(int16_t *X, int16_t *Y, int16_t mid, int N)
     int16_t rgain = c_rsqrt_norm(t);
     if (kl < 7) kl = 7;
     if (kr < 7) kr = 7;
-    for (int j = 0; j < N; j++) {
+    LFOR(L, j, 0, N) {
         int16_t l = (int16_t)c_mul16_p15(mid, X[j]);
         int16_t r = Y[j];
         X[j] = (int16_t)c_pshr(c_mul16(lgain, (int16_t)(l - r)), kl + 1);
         Y[j] = (int16_t)c_pshr(c_mul16(rgain, (int16_t)(l + r)), kr + 1);
     }
+    lsync(L);
 }
 
 DNI unsigned quant_band_stereo(BandCtx *ctx, int16_t *X, int16_t *Y, int N, int b, int B, int16_t *lowband,
@@ -1467,7 +1479,7 @@ DNI unsigned quant_band_stereo(BandCtx *ctx, int16_t *X, int16_t *Y, int N, int 
             cm |= quant_band(ctx, X, N, mbits, B, lowband, LM, lowband_out, 32767, lowband_scratch, fill);
         }
     }
-    if (N != 2) stereo_merge(X, Y, mid, N);
+    if (N != 2) stereo_merge(ctx->L, X, Y, mid, N);
     if (inv)
         for (int j = 0; j < N; j++) Y[j] = (int16_t)-Y[j];
     return cm;
@@ -1496,6 +1508,7 @@ DNI void quant_all_bands_dec(Lanes L, int start, int end, int16_t *X_, int16_t *
     ctx.disable_inv = disable_inv;
     ctx.avoid_split_noise = B > 1;
     ctx.w = w;
+    ctx.L = L;
     for (int i = start; i < end; i++) {
         int effective_lowband = -1;
         unsigned x_cm, y_cm;
@@ -1581,7 +1594,8 @@ DNI void quant_all_bands_dec(Lanes L, int start, int end, int16_t *X_, int16_t *
 }
 
 // celt/bands.c anti_collapse
-DNI void anti_collapse(int16_t *X_, const uint8_t *collapse_masks, int LM, int C, int size, int start, int end,
+DNI void anti_collapse(Lanes L, int16_t *X_, const uint8_t *collapse_masks, int LM, int C, int size, int start,
+                       int end,
                        const int16_t *logE, const int16_t *prev1logE, const int16_t *prev2logE,
                        const int32_t *pulses, uint32_t seed)
 {
@@ -1624,7 +1638,7 @@ DNI void anti_collapse(int16_t *X_, const uint8_t *collapse_masks, int LM, int C
                     renormalize = 1;
                 }
             }
-            if (renormalize) renormalise_vector(X, N0 << LM, 32767);
+            if (renormalize) renormalise_vector(L, X, N0 << LM, 32767);
         }
     }
 }
@@ -1966,7 +1980,7 @@ DNI void celt_decode_lost(Lanes L, CeltDec *st, int N, int LM, CeltScratch *w)
                     seed = c_lcg_rand(seed);
                     X[boffs + j] = (int16_t)((int32_t)seed >> 20);
                 }
-                renormalise_vector(X + boffs, blen, 32767);
+                renormalise_vector(L, X + boffs, blen, 32767);
             }
         }
         st->rng = seed;
@@ -2231,7 +2245,7 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
     if (anti_collapse_rsv > 0) anti_collapse_on = (int)rd_bits(dec, 1);
     unquant_energy_finalise(start, end, oldBandE, fine_quant, fine_priority, len * 8 - rd_tell(dec), dec, C);
     if (anti_collapse_on)
-        anti_collapse(X, w->collapse_masks, LM, C, N, start, end, oldBandE, oldLogE, oldLogE2, pulses, st->rng);
+        anti_collapse(L, X, w->collapse_masks, LM, C, N, start, end, oldBandE, oldLogE, oldLogE2, pulses, st->rng);
     if (silence)
         for (int i = 0; i < C * CELT_NB; i++) oldBandE[i] = -28672;   // -QCONST16(28.f, DB_SHIFT)
     if (st->prefilter_and_fold) prefilter_and_fold(st, N, w);
