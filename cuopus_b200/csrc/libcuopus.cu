@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <functional>
 #include <mutex>
 #include <numeric>
 #include <string>
@@ -412,10 +413,20 @@ int decode_batch(const cuopus_batch *b, cudaStream_t st, float *kernel_ms, Err &
 }
 
 // One call's worth of files merged into a single chain table.
+// std::allocator that leaves new elements uninitialised (the merged tables
+// are written in full right after they are sized).
+template <class T> struct NoInit : std::allocator<T> {
+    template <class U> struct rebind { using other = NoInit<U>; };
+    NoInit() = default;
+    template <class U> NoInit(const NoInit<U> &) {}
+    template <class U> void construct(U *p) noexcept { ::new ((void *)p) U; }
+    template <class U, class... A> void construct(U *p, A &&...a) { ::new ((void *)p) U(std::forward<A>(a)...); }
+};
+
 struct Plan {
-    std::vector<uint8_t> blob;
-    std::vector<uint64_t> off;
-    std::vector<uint32_t> len;
+    std::vector<uint8_t, NoInit<uint8_t>> blob;
+    std::vector<uint64_t, NoInit<uint64_t>> off;
+    std::vector<uint32_t, NoInit<uint32_t>> len;
     std::vector<uint32_t> first, npkts;
     std::vector<uint8_t> chans;
     std::vector<uint64_t> trim, keep, out_off, cap;
@@ -449,7 +460,7 @@ void plan_one(const uint8_t *ogg, size_t n, double seg_s, double preroll_ms, boo
     }
 }
 
-// Demux every file and merge the tables.  The files are demuxed on
+// Demux every file and merge the tables.  The files are demuxed and merged on
 // CUOPUS_DEMUX_THREADS host threads (default 1: the calling thread only, as
 // the reference's library, which starts no threads); errors are reported for
 // the lowest-numbered failing file, whatever the thread count.
@@ -467,51 +478,86 @@ int plan_files(const uint8_t *const *oggs, const size_t *ns, int nfiles, bool re
         for (int f; (f = next.fetch_add(1)) < nfiles;)
             plan_one(oggs[f], ns[f], seg_s, preroll_ms, require_mono, F[f]);
     };
-    std::vector<std::thread> pool;
-    for (int t = 1; t < nthreads; t++) {
-        try {
-            pool.emplace_back(work);
-        } catch (...) {
-            break;   // fewer threads; the calling thread does the rest
+    auto run = [&](const std::function<void()> &fn) {
+        next = 0;
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nthreads; t++) {
+            try {
+                pool.emplace_back(fn);
+            } catch (...) {
+                break;   // fewer threads; the calling thread does the rest
+            }
         }
-    }
-    work();
-    for (auto &t : pool) t.join();
+        fn();
+        for (auto &t : pool) t.join();
+    };
+    run(work);
+    // sizes and errors, file by file (the first failing file is reported)
+    std::vector<uint64_t> pkt0(nfiles + 1, 0), byte0(nfiles + 1, 0), ch0(nfiles + 1, 0);
+    P.file_out0.resize(nfiles);
+    P.file_keep.resize(nfiles);
+    P.file_chans.resize(nfiles);
+    P.file_play48.resize(nfiles);
     for (int f = 0; f < nfiles; f++) {
         FilePlan &Fp = F[f];
         if (!Fp.ok) {
             if (nfiles > 1) return err.set(RC_SOFT, "file %d: %s", f, Fp.e.c_str());
             return err.set(RC_SOFT, "%s", Fp.e.c_str());
         }
-        const cuo_host::Demux &d = Fp.d;
         const cuo_host::Chains &c = Fp.c;
-        uint64_t pkt_base = P.len.size(), data_base = P.blob.size();
-        P.blob.insert(P.blob.end(), d.blob.begin(), d.blob.end());
-        for (uint32_t k = 0; k < d.n_packets(); k++) {
-            P.off.push_back(d.off[k] + data_base);
-            P.len.push_back(d.len[k]);
-        }
         uint64_t fkeep = 0;
-        P.file_out0.push_back(P.out_elems);
         for (uint32_t i = 0; i < c.size(); i++) {
-            uint64_t capn = Fp.capn[i];
-            if (capn < (uint64_t)c.trim[i] + c.keep[i])
+            if (Fp.capn[i] < (uint64_t)c.trim[i] + c.keep[i])
                 return err.set(RC_SOFT, "chain %u capacity %llu < trim %u + keep %u", i,
-                               (unsigned long long)capn, c.trim[i], c.keep[i]);
-            P.first.push_back(c.first[i] + (uint32_t)pkt_base);
-            P.npkts.push_back(c.npkts[i]);
-            P.chans.push_back((uint8_t)d.channels);
-            P.trim.push_back(c.trim[i]);
-            P.keep.push_back(c.keep[i]);
-            P.out_off.push_back(P.out_elems + fkeep * d.channels);
-            P.cap.push_back(capn);
+                               (unsigned long long)Fp.capn[i], c.trim[i], c.keep[i]);
             fkeep += c.keep[i];
         }
-        P.file_keep.push_back(fkeep);
-        P.file_chans.push_back(d.channels);
-        P.file_play48.push_back(d.play48);
-        P.out_elems += fkeep * d.channels;
+        pkt0[f + 1] = pkt0[f] + Fp.d.n_packets();
+        byte0[f + 1] = byte0[f] + Fp.d.blob.size();
+        ch0[f + 1] = ch0[f] + c.size();
+        P.file_out0[f] = P.out_elems;
+        P.file_keep[f] = fkeep;
+        P.file_chans[f] = Fp.d.channels;
+        P.file_play48[f] = Fp.d.play48;
+        P.out_elems += fkeep * (uint64_t)Fp.d.channels;
     }
+    // merged tables: every file fills its own ranges (on the same threads)
+    P.blob.resize(byte0[nfiles]);
+    P.off.resize(pkt0[nfiles]);
+    P.len.resize(pkt0[nfiles]);
+    size_t nch = ch0[nfiles];
+    P.first.resize(nch);
+    P.npkts.resize(nch);
+    P.chans.resize(nch);
+    P.trim.resize(nch);
+    P.keep.resize(nch);
+    P.out_off.resize(nch);
+    P.cap.resize(nch);
+    run([&]() {
+        for (int f; (f = next.fetch_add(1)) < nfiles;) {
+            FilePlan &Fp = F[f];
+            const cuo_host::Demux &d = Fp.d;
+            const cuo_host::Chains &c = Fp.c;
+            if (!d.blob.empty()) memcpy(P.blob.data() + byte0[f], d.blob.data(), d.blob.size());
+            for (uint32_t k = 0; k < d.n_packets(); k++) {
+                P.off[pkt0[f] + k] = d.off[k] + byte0[f];
+                P.len[pkt0[f] + k] = d.len[k];
+            }
+            uint64_t fkeep = 0;
+            for (uint32_t i = 0; i < c.size(); i++) {
+                size_t j = ch0[f] + i;
+                P.first[j] = c.first[i] + (uint32_t)pkt0[f];
+                P.npkts[j] = c.npkts[i];
+                P.chans[j] = (uint8_t)d.channels;
+                P.trim[j] = c.trim[i];
+                P.keep[j] = c.keep[i];
+                P.out_off[j] = P.file_out0[f] + fkeep * d.channels;
+                P.cap[j] = Fp.capn[i];
+                fkeep += c.keep[i];
+            }
+            Fp = FilePlan();   // release this file's tables on this thread
+        }
+    });
     return RC_OK;
 }
 
