@@ -101,7 +101,7 @@ DNI void celt_reset(CeltDec *st)
     memset(st->lpc, 0, sizeof(st->lpc));
     memset(st->oldBandE, 0, sizeof(st->oldBandE));
     memset(st->backgroundLogE, 0, sizeof(st->backgroundLogE));
-    for (int i = 0; i < 2 * CELT_NB; i++) st->oldLogE[i] = st->oldLogE2[i] = -28 << 10;
+    for (int i = 0; i < 2 * CELT_NB; i++) st->oldLogE[i] = st->oldLogE2[i] = -28672;   // -QCONST16(28.f, DB_SHIFT)
     st->skip_plc = 1;
 }
 
