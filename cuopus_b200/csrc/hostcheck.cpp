@@ -100,6 +100,15 @@ unsigned long hc_slot_bytes(void) { return sizeof(cuo::ChainSlot); }
 // schedules through libopus (oref_ec_schedule, oref_ec_schedule2).
 extern "C" {
 
+// The decoder's PVQ codeword decode (rd_uint of V(n, k), then cwrsi) on a
+// buffer written by libopus's encode_pulses; y receives n pulses.
+void hc_pvq_decode(const uint8_t *buf, uint32_t len, int n, int k, int32_t *y)
+{
+    cuo::RangeDec d;
+    cuo::rd_init(&d, buf, len);
+    cuo::cwrsi(n, k, cuo::rd_uint(&d, cuo::pvq_v(n, k)), y);
+}
+
 void hc_ec_schedule(const uint8_t *buf, uint32_t len, uint32_t *out)
 {
     static const uint8_t icdf_tab[8] = {120, 112, 96, 64, 32, 16, 8, 0};

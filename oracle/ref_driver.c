@@ -288,3 +288,26 @@ void oref_ec_schedule2(const uint8_t *buf, uint32_t len, uint32_t *out)
     out[k++] = dec.rng;
     out[k++] = (uint32_t)dec.error;
 }
+
+/* ------------------------------------------------------------------ PVQ codewords */
+
+#include "entenc.h"
+#include "cwrs.h"
+
+/* celt/cwrs.c round trip: encode the pulse vector y (n entries, sum of
+ * magnitudes k) with encode_pulses into buf (cap bytes, the range coder's
+ * front and raw-bit tail both inside it), then decode it back with
+ * decode_pulses into y_out.  Returns 0, or the encoder's error flag. */
+int oref_pvq_roundtrip(int n, int k, const int *y, unsigned char *buf, uint32_t cap, int *y_out)
+{
+    ec_enc enc;
+    ec_dec dec;
+    memset(buf, 0, cap);
+    ec_enc_init(&enc, buf, cap);
+    encode_pulses(y, n, k, &enc);
+    ec_enc_done(&enc);
+    if (enc.error) return enc.error;
+    ec_dec_init(&dec, buf, cap);
+    decode_pulses(y_out, n, k, &dec);
+    return dec.error;
+}

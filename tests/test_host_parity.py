@@ -373,3 +373,47 @@ def test_parallel_demux_reports_like_the_sequential_one(cn, monkeypatch):
         assert rc == 1
         seen.add(err.value)
     assert len(seen) == 1 and next(iter(seen)).startswith(b"file 2:")
+
+
+def _pvq_v(n, k):
+    """Number of integer vectors of length n with magnitudes summing to k."""
+    from math import comb
+    return sum((1 << j) * comb(n, j) * comb(k - 1, j - 1) for j in range(1, min(n, k) + 1))
+
+
+def test_pvq_codewords_match_libopus(hc):
+    """CELT PVQ codewords (celt/cwrs.c): random pulse vectors, encoded by
+    libopus's encode_pulses, decode to the same vector through libopus's
+    decode_pulses and through the decoder's cwrsi (host build), over band
+    sizes 2-176 and pulse counts up to 30 within the codeword tables."""
+    lib = corpus.ref_lib()
+    lib.oref_pvq_roundtrip.restype = ctypes.c_int
+    rng = np.random.default_rng(17)
+    # (n, k) pairs whose codebook size fits 32 bits and lies inside the U table
+    # rows the decoder indexes (min(n, k + 1) <= 5 with n <= 160, or small n and k)
+    pairs = []
+    for n in list(range(2, 33)) + [40, 48, 64, 72, 88, 96, 128, 144, 160, 176]:
+        for k in range(1, 31):
+            if _pvq_v(n, k) >= 1 << 32:
+                continue
+            r = min(n, k + 1)
+            if (r <= 5 and max(n, k + 1) < 170) or (r <= 10 and max(n, k + 1) <= 20):
+                pairs.append((n, k))
+    checked = 0
+    buf = (ctypes.c_ubyte * 64)()
+    for n, k in pairs:
+        for _ in range(3):
+            y = np.zeros(n, np.int32)
+            for _ in range(k):
+                y[int(rng.integers(0, n))] += 1
+            y *= np.where(rng.random(n) < 0.5, -1, 1).astype(np.int32)
+            yin = np.ascontiguousarray(y, np.int32)
+            yref = np.zeros(n, np.int32)
+            assert lib.oref_pvq_roundtrip(n, k, yin.ctypes.data_as(ctypes.c_void_p), buf, 64,
+                                          yref.ctypes.data_as(ctypes.c_void_p)) == 0
+            assert np.array_equal(yref, yin), (n, k)
+            got = np.zeros(n, np.int32)
+            hc.hc_pvq_decode(buf, 64, n, k, got.ctypes.data_as(ctypes.c_void_p))
+            assert np.array_equal(got, yin), (n, k, yin, got)
+            checked += 1
+    assert checked > 600
