@@ -109,6 +109,14 @@ void hc_pvq_decode(const uint8_t *buf, uint32_t len, int n, int k, int32_t *y)
     cuo::cwrsi(n, k, cuo::rd_uint(&d, cuo::pvq_v(n, k)), y);
 }
 
+// The decoder's inverse MDCT (pre-rotation, FFT, post-rotation, TDAC
+// mirror) for one block: the contract of clt_mdct_backward_c.
+void hc_imdct(const int32_t *in, int32_t *out, int shift, int stride)
+{
+    cuo::Lanes L{0, 1, 1u};
+    cuo::mdct_backward(L, in, out, shift, stride);
+}
+
 void hc_ec_schedule(const uint8_t *buf, uint32_t len, uint32_t *out)
 {
     static const uint8_t icdf_tab[8] = {120, 112, 96, 64, 32, 16, 8, 0};

@@ -311,3 +311,21 @@ int oref_pvq_roundtrip(int n, int k, const int *y, unsigned char *buf, uint32_t 
     decode_pulses(y_out, n, k, &dec);
     return dec.error;
 }
+
+/* ------------------------------------------------------------------ inverse MDCT */
+
+#include "modes.h"
+#include "mdct.h"
+
+/* celt/mdct.c clt_mdct_backward_c of the 48 kHz / 960-sample mode (the one
+ * the decoder uses) on in[] with the given shift (0 = 20 ms ... 3 = 2.5 ms)
+ * and stride (short blocks); out[] holds the overlap history on entry, as in
+ * celt_synthesis.  Returns 0, or -1 when the mode is unavailable. */
+int oref_imdct(const int32_t *in, int32_t *out, int shift, int stride)
+{
+    int err = 0;
+    const CELTMode *m = opus_custom_mode_create(48000, 960, &err);
+    if (!m || err) return -1;
+    clt_mdct_backward_c(&m->mdct, (kiss_fft_scalar *)in, out, m->window, m->overlap, shift, stride, 0);
+    return 0;
+}

@@ -417,3 +417,30 @@ def test_pvq_codewords_match_libopus(hc):
             assert np.array_equal(got, yin), (n, k, yin, got)
             checked += 1
     assert checked > 600
+
+
+def test_imdct_matches_libopus(hc):
+    """The decoder's inverse MDCT against libopus's clt_mdct_backward_c of the
+    48 kHz mode: every block size (shift 0-3) and the short-block strides,
+    random coefficients, random overlap history; every output word equal."""
+    lib = corpus.ref_lib()
+    lib.oref_imdct.restype = ctypes.c_int
+    rng = np.random.default_rng(23)
+    n_mdct, overlap = 1920, 120
+    checked = 0
+    # the decoder's calls: long blocks of every size (shift 3 - LM, stride 1)
+    # and the short blocks of transient frames (shift 3, stride 1 << LM)
+    for shift, stride in [(0, 1), (1, 1), (2, 1), (3, 1), (3, 2), (3, 4), (3, 8)]:
+        for trial in range(12):
+            scale = 1 << int(rng.integers(8, 22))
+            x = rng.integers(-scale, scale, n_mdct, dtype=np.int64).astype(np.int32)
+            hist = rng.integers(-scale, scale, overlap, dtype=np.int64).astype(np.int32)
+            want = np.zeros(n_mdct + overlap, np.int32)
+            want[:overlap] = hist
+            got = want.copy()
+            assert lib.oref_imdct(x.ctypes.data_as(ctypes.c_void_p), want.ctypes.data_as(ctypes.c_void_p),
+                                  shift, stride) == 0
+            hc.hc_imdct(x.ctypes.data_as(ctypes.c_void_p), got.ctypes.data_as(ctypes.c_void_p), shift, stride)
+            assert np.array_equal(got, want), (shift, stride, trial)
+            checked += 1
+    assert checked == 7 * 12
