@@ -117,6 +117,45 @@ void hc_imdct(const int32_t *in, int32_t *out, int shift, int stride)
     cuo::mdct_backward(L, in, out, shift, stride);
 }
 
+// SILK NLSF to LPC conversion of the decoder.
+void hc_nlsf2a(int16_t *a_Q12, const int16_t *nlsf, int d)
+{
+    cuo::SilkWork sw;
+    cuo::silk_nlsf2a(a_Q12, nlsf, d, &sw);
+}
+
+// The decoder's SILK resampler to 48 kHz (all-pass up2 + FIR interpolation),
+// `frame` input samples per call; returns the output samples written.
+int hc_silk_resample(int fs_in, const int16_t *in, int n_in, int frame, int16_t *out)
+{
+    cuo::Lanes L{0, 1, 1u};
+    cuo::SilkResampler S;
+    int16_t buf[2 * 160 + 8];
+    cuo::silk_resampler_init48(&S, fs_in);
+    int o = 0;
+    for (int i = 0; i + frame <= n_in; i += frame) {
+        cuo::silk_resample(L, &S, out + o, in + i, frame, buf);
+        o += frame * (48000 / fs_in);
+    }
+    return o;
+}
+
+// The decoder's comb (post-)filter in place on buf + off: the serial form
+// (lanes = 0) or the block-parallel form the decoder runs (lanes = 1, here
+// with a single lane walking the same blocks).
+void hc_comb_filter(int32_t *buf, int off, int T0, int T1, int N, int g0, int g1, int tapset0, int tapset1,
+                    int lanes)
+{
+    if (lanes) {
+        cuo::Lanes L{0, 1, 1u};
+        cuo::comb_filter_lanes(L, buf + off, buf + off, T0, T1, N, (int16_t)g0, (int16_t)g1, tapset0, tapset1,
+                               cuo::T_celt_window, cuo::CELT_OVERLAP);
+    } else {
+        cuo::comb_filter(buf + off, buf + off, T0, T1, N, (int16_t)g0, (int16_t)g1, tapset0, tapset1,
+                         cuo::T_celt_window, cuo::CELT_OVERLAP);
+    }
+}
+
 void hc_ec_schedule(const uint8_t *buf, uint32_t len, uint32_t *out)
 {
     static const uint8_t icdf_tab[8] = {120, 112, 96, 64, 32, 16, 8, 0};

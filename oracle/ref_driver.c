@@ -329,3 +329,40 @@ int oref_imdct(const int32_t *in, int32_t *out, int shift, int stride)
     clt_mdct_backward_c(&m->mdct, (kiss_fft_scalar *)in, out, m->window, m->overlap, shift, stride, 0);
     return 0;
 }
+
+/* ------------------------------------------------------------------ SILK / CELT components */
+
+#include "SigProc_FIX.h"
+#include "celt.h"
+
+/* silk/NLSF2A.c: NLSF (Q15, d of them) to LPC coefficients (Q12). */
+void oref_nlsf2a(int16_t *a_Q12, const int16_t *nlsf, int d)
+{
+    silk_NLSF2A(a_Q12, nlsf, d, 0);
+}
+
+/* silk/resampler.c from fs_in to 48 kHz, the decoder's set-up, fed `frame`
+ * input samples per call for n_in samples: out receives n_in * 48000 / fs_in. */
+int oref_silk_resample(int fs_in, const int16_t *in, int n_in, int frame, int16_t *out)
+{
+    silk_resampler_state_struct S;
+    if (silk_resampler_init(&S, fs_in, 48000, 0)) return -1;
+    int o = 0;
+    for (int i = 0; i + frame <= n_in; i += frame) {
+        if (silk_resampler(&S, out + o, in + i, frame)) return -2;
+        o += frame * (48000 / fs_in);
+    }
+    return o;
+}
+
+/* celt/celt.c comb_filter in place on buf + off (the history before it is
+ * read), with the 48 kHz mode's window and overlap. */
+int oref_comb_filter(int32_t *buf, int off, int T0, int T1, int N, int g0, int g1, int tapset0, int tapset1)
+{
+    int err = 0;
+    const CELTMode *m = opus_custom_mode_create(48000, 960, &err);
+    if (!m || err) return -1;
+    comb_filter(buf + off, buf + off, T0, T1, N, (opus_val16)g0, (opus_val16)g1, tapset0, tapset1, m->window,
+                m->overlap, 0);
+    return 0;
+}

@@ -444,3 +444,66 @@ def test_imdct_matches_libopus(hc):
             assert np.array_equal(got, want), (shift, stride, trial)
             checked += 1
     assert checked == 7 * 12
+
+
+def test_nlsf2a_matches_libopus(hc):
+    """SILK NLSF to LPC (silk/NLSF2A.c, with its bandwidth-expansion loop for
+    unstable filters) on random increasing NLSF vectors of order 10 and 16."""
+    lib = corpus.ref_lib()
+    rng = np.random.default_rng(29)
+    for trial in range(400):
+        d = 16 if trial % 2 else 10
+        gap = int(rng.integers(1, 400))
+        v = np.sort(rng.integers(1, 32767 - gap * d, d)) + gap * np.arange(1, d + 1)
+        nlsf = np.ascontiguousarray(np.clip(v, 1, 32766).astype(np.int16))
+        want = np.zeros(d, np.int16)
+        got = np.zeros(d, np.int16)
+        lib.oref_nlsf2a(want.ctypes.data_as(ctypes.c_void_p), nlsf.ctypes.data_as(ctypes.c_void_p), d)
+        hc.hc_nlsf2a(got.ctypes.data_as(ctypes.c_void_p), nlsf.ctypes.data_as(ctypes.c_void_p), d)
+        assert np.array_equal(got, want), (trial, nlsf)
+
+
+@pytest.mark.parametrize("fs_in", [8000, 12000, 16000])
+def test_silk_resampler_matches_libopus(hc, fs_in):
+    """The SILK decoder's resampler to 48 kHz (silk/resampler.c, IIR_FIR: up2
+    all-pass + fractional FIR) over a stream fed frame by frame: 10 and 20 ms
+    frames of noise, tones and full-scale steps, every output sample equal."""
+    lib = corpus.ref_lib()
+    rng = np.random.default_rng(fs_in)
+    n = fs_in * 2
+    t = np.arange(n)
+    x = (8000 * np.sin(2 * np.pi * 440 * t / fs_in) + rng.normal(0, 3000, n)).astype(np.int64)
+    x[n // 3:n // 3 + 50] = 32767
+    x[n // 2:n // 2 + 50] = -32768
+    x = np.ascontiguousarray(np.clip(x, -32768, 32767).astype(np.int16))
+    for ms in (10, 20):
+        frame = fs_in * ms // 1000
+        want = np.zeros(n * (48000 // fs_in), np.int16)
+        got = np.zeros_like(want)
+        a = lib.oref_silk_resample(fs_in, x.ctypes.data_as(ctypes.c_void_p), n, frame,
+                                   want.ctypes.data_as(ctypes.c_void_p))
+        b = hc.hc_silk_resample(fs_in, x.ctypes.data_as(ctypes.c_void_p), n, frame,
+                                got.ctypes.data_as(ctypes.c_void_p))
+        assert a == b > 0
+        assert np.array_equal(got, want), (fs_in, ms)
+
+
+@pytest.mark.parametrize("lanes", [0, 1])
+def test_comb_filter_matches_libopus(hc, lanes):
+    """The CELT comb (post-)filter (celt/celt.c comb_filter, in place, the
+    decoder's use) in the serial form and in the block-parallel form: random
+    pitch periods 15-1022 across the cross-fade, gains and tapsets, 2.5-20 ms."""
+    lib = corpus.ref_lib()
+    rng = np.random.default_rng(31 + lanes)
+    off = 1100
+    for trial in range(300):
+        N = int(rng.choice([120, 240, 480, 960]))
+        T0, T1 = (int(v) for v in rng.integers(15, 1023, 2))
+        g0, g1 = (int(3072 * v) for v in rng.integers(0, 9, 2))
+        t0, t1 = (int(v) for v in rng.integers(0, 3, 2))
+        buf = rng.integers(-1 << 22, 1 << 22, off + N, dtype=np.int64).astype(np.int32)
+        want = np.ascontiguousarray(buf.copy())
+        got = np.ascontiguousarray(buf.copy())
+        assert lib.oref_comb_filter(want.ctypes.data_as(ctypes.c_void_p), off, T0, T1, N, g0, g1, t0, t1) == 0
+        hc.hc_comb_filter(got.ctypes.data_as(ctypes.c_void_p), off, T0, T1, N, g0, g1, t0, t1, lanes)
+        assert np.array_equal(got, want), (trial, N, T0, T1, g0, g1, t0, t1)
