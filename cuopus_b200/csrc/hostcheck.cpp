@@ -156,6 +156,32 @@ void hc_comb_filter(int32_t *buf, int off, int T0, int T1, int N, int g0, int g1
     }
 }
 
+// The decoder's CELT bit allocation (clt_compute_allocation, decode mode)
+// with its caps, same output layout as the oracle's oref_alloc.
+int hc_alloc(const uint8_t *buf, uint32_t len, int start, int end, const int32_t *offsets, int alloc_trim,
+             int32_t total, int C, int LM, int32_t *out)
+{
+    static thread_local cuo::CeltScratch w;
+    int32_t cap[21], pulses[21] = {}, ebits[21] = {}, fine_priority[21] = {}, balance = 0;
+    int intensity = 0, dual_stereo = 0;
+    cuo::RangeDec d;
+    cuo::init_caps(cap, LM, C);
+    cuo::rd_init(&d, buf, len);
+    int coded = cuo::clt_compute_allocation(start, end, offsets, cap, alloc_trim, &intensity, &dual_stereo, total,
+                                            &balance, pulses, ebits, fine_priority, C, LM, &d, &w);
+    int k = 0;
+    out[k++] = coded;
+    out[k++] = intensity;
+    out[k++] = dual_stereo;
+    out[k++] = balance;
+    for (int i = 0; i < 21; i++) out[k++] = pulses[i];
+    for (int i = 0; i < 21; i++) out[k++] = ebits[i];
+    for (int i = 0; i < 21; i++) out[k++] = fine_priority[i];
+    out[k++] = (int32_t)cuo::rd_tell_frac(&d);
+    out[k++] = (int32_t)d.rng;
+    return 0;
+}
+
 void hc_ec_schedule(const uint8_t *buf, uint32_t len, uint32_t *out)
 {
     static const uint8_t icdf_tab[8] = {120, 112, 96, 64, 32, 16, 8, 0};

@@ -366,3 +366,34 @@ int oref_comb_filter(int32_t *buf, int off, int T0, int T1, int N, int g0, int g
                 m->overlap, 0);
     return 0;
 }
+
+#include "rate.h"
+
+/* celt/rate.c clt_compute_allocation in decode mode (bits read from a range
+ * decoder over buf) for the 48 kHz mode, caps from celt/celt.c init_caps.
+ * out: codedBands, intensity, dual_stereo, balance, then pulses[21],
+ * ebits[21], fine_priority[21], then the decoder's tell_frac and rng. */
+int oref_alloc(const uint8_t *buf, uint32_t len, int start, int end, const int *offsets, int alloc_trim,
+               int32_t total, int C, int LM, int32_t *out)
+{
+    int err = 0, cap[21], pulses[21] = {0}, ebits[21] = {0}, fine_priority[21] = {0}, intensity = 0, dual_stereo = 0;
+    opus_int32 balance = 0;
+    ec_dec dec;
+    const CELTMode *m = opus_custom_mode_create(48000, 960, &err);
+    if (!m || err) return -1;
+    init_caps(m, cap, LM, C);
+    ec_dec_init(&dec, (unsigned char *)buf, len);
+    int coded = clt_compute_allocation(m, start, end, offsets, cap, alloc_trim, &intensity, &dual_stereo, total,
+                                       &balance, pulses, ebits, fine_priority, C, LM, &dec, 0, 0, 0);
+    int k = 0;
+    out[k++] = coded;
+    out[k++] = intensity;
+    out[k++] = dual_stereo;
+    out[k++] = balance;
+    for (int i = 0; i < 21; i++) out[k++] = pulses[i];
+    for (int i = 0; i < 21; i++) out[k++] = ebits[i];
+    for (int i = 0; i < 21; i++) out[k++] = fine_priority[i];
+    out[k++] = (int32_t)ec_tell_frac(&dec);
+    out[k++] = (int32_t)dec.rng;
+    return 0;
+}

@@ -507,3 +507,30 @@ def test_comb_filter_matches_libopus(hc, lanes):
         assert lib.oref_comb_filter(want.ctypes.data_as(ctypes.c_void_p), off, T0, T1, N, g0, g1, t0, t1) == 0
         hc.hc_comb_filter(got.ctypes.data_as(ctypes.c_void_p), off, T0, T1, N, g0, g1, t0, t1, lanes)
         assert np.array_equal(got, want), (trial, N, T0, T1, g0, g1, t0, t1)
+
+
+def test_celt_allocation_matches_libopus(hc):
+    """CELT bit allocation (celt/rate.c clt_compute_allocation in decode mode,
+    caps from init_caps): random budgets, trims, dynalloc boosts, band ranges
+    (CELT and hybrid), mono and stereo, every frame size; the decisions it
+    reads from the range decoder come from random bytes.  Coded bands,
+    intensity, dual stereo, balance, pulses, fine bits and priorities, and the
+    range decoder's state after it all equal."""
+    lib = corpus.ref_lib()
+    rng = np.random.default_rng(37)
+    out_w = np.zeros(4 + 63 + 2, np.int32)
+    out_g = np.zeros_like(out_w)
+    for trial in range(1500):
+        start = 17 if trial % 4 == 0 else 0
+        end = int(rng.choice([13, 17, 19, 21])) if start == 0 else int(rng.choice([19, 21]))
+        C, LM = 1 + int(rng.integers(0, 2)), int(rng.integers(0, 4))
+        trim = int(rng.integers(0, 11))
+        total = int(rng.integers(0, 8 * 8 * 300))
+        offsets = np.zeros(21, np.int32)
+        for i in rng.integers(start, end, int(rng.integers(0, 4))):
+            offsets[i] = int(rng.integers(1, 4)) * 8 * C
+        buf = (ctypes.c_ubyte * 160)(*rng.integers(0, 256, 160).tolist())
+        args = (buf, 160, start, end, offsets.ctypes.data_as(ctypes.c_void_p), trim, total, C, LM)
+        assert lib.oref_alloc(*args, out_w.ctypes.data_as(ctypes.c_void_p)) == 0
+        hc.hc_alloc(*args, out_g.ctypes.data_as(ctypes.c_void_p))
+        assert np.array_equal(out_g, out_w), (trial, start, end, C, LM, trim, total)
