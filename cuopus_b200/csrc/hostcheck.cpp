@@ -182,6 +182,37 @@ int hc_alloc(const uint8_t *buf, uint32_t len, int start, int end, const int32_t
     return 0;
 }
 
+// Allocation then the decoder's band decoding (quant_all_bands_dec), the
+// oracle's oref_bands layout.
+int hc_bands(const uint8_t *buf, uint32_t len, int start, int end, const int32_t *offsets, int alloc_trim, int C,
+             int LM, int shortBlocks, int spread, const int32_t *tf_res, int disable_inv, uint32_t seed,
+             int16_t *X_out, uint8_t *cm_out, uint32_t *tail)
+{
+    static thread_local cuo::CeltScratch w;
+    cuo::Lanes L{0, 1, 1u};
+    int32_t cap[21], pulses[21] = {}, ebits[21] = {}, fine_priority[21] = {}, balance = 0;
+    int intensity = 0, dual_stereo = 0;
+    int N = 120 << LM;
+    memset(w.X, 0, sizeof w.X);
+    memset(w.collapse_masks, 0, sizeof w.collapse_masks);
+    cuo::RangeDec d;
+    cuo::init_caps(cap, LM, C);
+    cuo::rd_init(&d, buf, len);
+    int32_t bits = (int32_t)(len * 8 << 3) - (int32_t)cuo::rd_tell_frac(&d) - 1;
+    int coded = cuo::clt_compute_allocation(start, end, offsets, cap, alloc_trim, &intensity, &dual_stereo, bits,
+                                            &balance, pulses, ebits, fine_priority, C, LM, &d, &w);
+    uint32_t s = seed;
+    cuo::quant_all_bands_dec(L, start, end, w.X, C == 2 ? w.X + N : nullptr, w.collapse_masks, pulses, shortBlocks,
+                             spread, dual_stereo, intensity, tf_res, (int32_t)(len * (8 << 3)), balance, &d, LM,
+                             coded, &s, disable_inv, &w);
+    memcpy(X_out, w.X, sizeof(int16_t) * C * N);
+    memcpy(cm_out, w.collapse_masks, (size_t)C * 21);
+    tail[0] = s;
+    tail[1] = cuo::rd_tell_frac(&d);
+    tail[2] = d.rng;
+    return 0;
+}
+
 void hc_ec_schedule(const uint8_t *buf, uint32_t len, uint32_t *out)
 {
     static const uint8_t icdf_tab[8] = {120, 112, 96, 64, 32, 16, 8, 0};

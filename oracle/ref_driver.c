@@ -397,3 +397,41 @@ int oref_alloc(const uint8_t *buf, uint32_t len, int start, int end, const int *
     out[k++] = (int32_t)dec.rng;
     return 0;
 }
+
+#include "bands.h"
+
+/* Allocation then celt/bands.c quant_all_bands in decode mode, on one range
+ * decoder over buf (len bytes, the whole packet budget), as celt_decode_with_ec
+ * runs them: X_out receives the C * (120 << LM) normalised coefficients,
+ * cm_out the C * 21 collapse masks, tail the seed, tell_frac and rng. */
+int oref_bands(const uint8_t *buf, uint32_t len, int start, int end, const int *offsets, int alloc_trim, int C,
+               int LM, int shortBlocks, int spread, const int *tf_res, int disable_inv, uint32_t seed,
+               int16_t *X_out, uint8_t *cm_out, uint32_t *tail)
+{
+    int err = 0, cap[21], pulses[21] = {0}, ebits[21] = {0}, fine_priority[21] = {0}, intensity = 0,
+        dual_stereo = 0;
+    opus_int32 balance = 0;
+    celt_norm X[2 * 960];
+    unsigned char masks[2 * 21];
+    ec_dec dec;
+    const CELTMode *m = opus_custom_mode_create(48000, 960, &err);
+    if (!m || err) return -1;
+    int N = 120 << LM;
+    memset(X, 0, sizeof X);
+    memset(masks, 0, sizeof masks);
+    init_caps(m, cap, LM, C);
+    ec_dec_init(&dec, (unsigned char *)buf, len);
+    opus_int32 bits = (opus_int32)(len * 8 << 3) - (opus_int32)ec_tell_frac(&dec) - 1;
+    int coded = clt_compute_allocation(m, start, end, offsets, cap, alloc_trim, &intensity, &dual_stereo, bits,
+                                       &balance, pulses, ebits, fine_priority, C, LM, &dec, 0, 0, 0);
+    opus_uint32 s = seed;
+    quant_all_bands(0, m, start, end, X, C == 2 ? X + N : NULL, masks, NULL, pulses, shortBlocks, spread,
+                    dual_stereo, intensity, (int *)tf_res, (opus_int32)(len * (8 << 3)), balance, &dec, LM, coded,
+                    &s, 0, 0, disable_inv);
+    memcpy(X_out, X, sizeof(int16_t) * C * N);
+    memcpy(cm_out, masks, (size_t)C * 21);
+    tail[0] = s;
+    tail[1] = ec_tell_frac(&dec);
+    tail[2] = dec.rng;
+    return 0;
+}

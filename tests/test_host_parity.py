@@ -534,3 +534,42 @@ def test_celt_allocation_matches_libopus(hc):
         assert lib.oref_alloc(*args, out_w.ctypes.data_as(ctypes.c_void_p)) == 0
         hc.hc_alloc(*args, out_g.ctypes.data_as(ctypes.c_void_p))
         assert np.array_equal(out_g, out_w), (trial, start, end, C, LM, trim, total)
+
+
+def test_celt_band_decoding_matches_libopus(hc):
+    """CELT band shapes (celt/bands.c quant_all_bands, decode mode, after the
+    allocation, on one range decoder over random bytes): PVQ codewords, theta
+    splits, folding and noise fill, stereo (intensity, dual, mid/side merge,
+    phase inversion on or off), transient short blocks with time-frequency
+    changes, every spread.  Every coefficient, collapse mask, the folding seed
+    and the range decoder's state equal."""
+    lib = corpus.ref_lib()
+    rng = np.random.default_rng(41)
+    for trial in range(1200):
+        start = 17 if trial % 5 == 0 else 0
+        end = int(rng.choice([13, 17, 19, 21])) if start == 0 else int(rng.choice([19, 21]))
+        C, LM = 1 + int(rng.integers(0, 2)), int(rng.integers(0, 4))
+        transient = LM > 0 and rng.random() < 0.3
+        shortBlocks = (1 << LM) if transient else 0
+        tf = np.zeros(21, np.int32)
+        if LM > 0 and rng.random() < 0.5:
+            tf[:] = rng.choice([0, 1] if transient else [0, -1], 21)
+        offsets = np.zeros(21, np.int32)
+        for i in rng.integers(start, end, int(rng.integers(0, 4))):
+            offsets[i] = int(rng.integers(1, 4)) * 8 * C
+        nbytes = int(rng.integers(8, 200))
+        buf = (ctypes.c_ubyte * nbytes)(*rng.integers(0, 256, nbytes).tolist())
+        spread, trim, inv = int(rng.integers(0, 4)), int(rng.integers(0, 11)), int(rng.integers(0, 2))
+        seed = int(rng.integers(0, 1 << 32))
+        outs = []
+        for f in (lib.oref_bands, hc.hc_bands):
+            X = np.zeros(2 * 960, np.int16)
+            cm = np.zeros(42, np.uint8)
+            tail = np.zeros(3, np.uint32)
+            f(buf, nbytes, start, end, offsets.ctypes.data_as(ctypes.c_void_p), trim, C, LM, shortBlocks, spread,
+              tf.ctypes.data_as(ctypes.c_void_p), inv, ctypes.c_uint32(seed), X.ctypes.data_as(ctypes.c_void_p),
+              cm.ctypes.data_as(ctypes.c_void_p), tail.ctypes.data_as(ctypes.c_void_p))
+            outs.append((X, cm, tail))
+        (Xw, cw, tw), (Xg, cg, tg) = outs
+        assert np.array_equal(Xg, Xw) and np.array_equal(cg, cw) and np.array_equal(tg, tw), \
+            (trial, start, end, C, LM, shortBlocks, spread, trim, inv)
