@@ -213,6 +213,28 @@ int hc_bands(const uint8_t *buf, uint32_t len, int start, int end, const int32_t
     return 0;
 }
 
+// The decoder's band-energy decoding around the allocation, the oracle's
+// oref_energy layout.
+int hc_energy(const uint8_t *buf, uint32_t len, int start, int end, int intra, const int32_t *offsets,
+              int alloc_trim, int C, int LM, int16_t *oldE, uint32_t *tail)
+{
+    static thread_local cuo::CeltScratch w;
+    int32_t cap[21], pulses[21] = {}, ebits[21] = {}, fine_priority[21] = {}, balance = 0;
+    int intensity = 0, dual_stereo = 0;
+    cuo::RangeDec d;
+    cuo::rd_init(&d, buf, len);
+    cuo::unquant_coarse_energy(start, end, oldE, intra, &d, C, LM);
+    cuo::init_caps(cap, LM, C);
+    int32_t bits = (int32_t)(len * 8 << 3) - (int32_t)cuo::rd_tell_frac(&d) - 1;
+    cuo::clt_compute_allocation(start, end, offsets, cap, alloc_trim, &intensity, &dual_stereo, bits, &balance,
+                                pulses, ebits, fine_priority, C, LM, &d, &w);
+    cuo::unquant_fine_energy(start, end, oldE, ebits, &d, C);
+    cuo::unquant_energy_finalise(start, end, oldE, ebits, fine_priority, (int)len * 8 - cuo::rd_tell(&d), &d, C);
+    tail[0] = cuo::rd_tell_frac(&d);
+    tail[1] = d.rng;
+    return 0;
+}
+
 void hc_ec_schedule(const uint8_t *buf, uint32_t len, uint32_t *out)
 {
     static const uint8_t icdf_tab[8] = {120, 112, 96, 64, 32, 16, 8, 0};

@@ -435,3 +435,32 @@ int oref_bands(const uint8_t *buf, uint32_t len, int start, int end, const int *
     tail[2] = dec.rng;
     return 0;
 }
+
+#include "quant_bands.h"
+
+/* The band energies of one frame as celt_decode_with_ec decodes them around
+ * the allocation: celt/quant_bands.c unquant_coarse_energy, then
+ * clt_compute_allocation, unquant_fine_energy and unquant_energy_finalise with
+ * the bits left.  oldE (2 x 21, Q8 log energies) is updated in place; tail
+ * receives tell_frac and rng. */
+int oref_energy(const uint8_t *buf, uint32_t len, int start, int end, int intra, const int *offsets,
+                int alloc_trim, int C, int LM, int16_t *oldE, uint32_t *tail)
+{
+    int err = 0, cap[21], pulses[21] = {0}, ebits[21] = {0}, fine_priority[21] = {0}, intensity = 0,
+        dual_stereo = 0;
+    opus_int32 balance = 0;
+    ec_dec dec;
+    const CELTMode *m = opus_custom_mode_create(48000, 960, &err);
+    if (!m || err) return -1;
+    ec_dec_init(&dec, (unsigned char *)buf, len);
+    unquant_coarse_energy(m, start, end, oldE, intra, &dec, C, LM);
+    init_caps(m, cap, LM, C);
+    opus_int32 bits = (opus_int32)(len * 8 << 3) - (opus_int32)ec_tell_frac(&dec) - 1;
+    clt_compute_allocation(m, start, end, offsets, cap, alloc_trim, &intensity, &dual_stereo, bits, &balance,
+                           pulses, ebits, fine_priority, C, LM, &dec, 0, 0, 0);
+    unquant_fine_energy(m, start, end, oldE, ebits, &dec, C);
+    unquant_energy_finalise(m, start, end, oldE, ebits, fine_priority, (int)len * 8 - ec_tell(&dec), &dec, C);
+    tail[0] = ec_tell_frac(&dec);
+    tail[1] = dec.rng;
+    return 0;
+}

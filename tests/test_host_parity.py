@@ -573,3 +573,32 @@ def test_celt_band_decoding_matches_libopus(hc):
         (Xw, cw, tw), (Xg, cg, tg) = outs
         assert np.array_equal(Xg, Xw) and np.array_equal(cg, cw) and np.array_equal(tg, tw), \
             (trial, start, end, C, LM, shortBlocks, spread, trim, inv)
+
+
+def test_celt_energy_decoding_matches_libopus(hc):
+    """CELT band energies (celt/quant_bands.c): coarse energy (Laplace-coded,
+    intra and inter prediction, every frame size), the allocation, fine energy
+    and the final bits, on random bytes from random previous energies, mono and
+    stereo; the energies and the range decoder's state equal."""
+    lib = corpus.ref_lib()
+    rng = np.random.default_rng(43)
+    for trial in range(1500):
+        start = 17 if trial % 5 == 0 else 0
+        end = int(rng.choice([13, 17, 19, 21])) if start == 0 else int(rng.choice([19, 21]))
+        C, LM, intra = 1 + int(rng.integers(0, 2)), int(rng.integers(0, 4)), int(rng.integers(0, 2))
+        offsets = np.zeros(21, np.int32)
+        for i in rng.integers(start, end, int(rng.integers(0, 4))):
+            offsets[i] = int(rng.integers(1, 4)) * 8 * C
+        nbytes = int(rng.integers(4, 200))
+        buf = (ctypes.c_ubyte * nbytes)(*rng.integers(0, 256, nbytes).tolist())
+        old = rng.integers(-28 << 8, 20 << 8, 42).astype(np.int16)
+        trim = int(rng.integers(0, 11))
+        res = []
+        for f in (lib.oref_energy, hc.hc_energy):
+            e = np.ascontiguousarray(old.copy())
+            tail = np.zeros(2, np.uint32)
+            f(buf, nbytes, start, end, intra, offsets.ctypes.data_as(ctypes.c_void_p), trim, C, LM,
+              e.ctypes.data_as(ctypes.c_void_p), tail.ctypes.data_as(ctypes.c_void_p))
+            res.append((e, tail))
+        assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1]), \
+            (trial, start, end, C, LM, intra)
