@@ -235,6 +235,44 @@ int hc_energy(const uint8_t *buf, uint32_t len, int start, int end, int intra, c
     return 0;
 }
 
+// The decoder's SILK entropy decoding (indices and pulses), the oracle's
+// oref_silk_entropy layout.
+int hc_silk_entropy(const uint8_t *buf, uint32_t len, int fs_kHz, int nb_subfr, int frames, const int32_t *vad,
+                    int cond_first, int32_t *out, uint32_t *tail)
+{
+    static thread_local cuo::SilkChan c;
+    static thread_local cuo::SilkScratch w;
+    cuo::silk_reset_chan(&c);
+    c.nb_subfr = nb_subfr;
+    cuo::silk_decoder_set_fs(&c, fs_kHz, 48000);
+    cuo::RangeDec d;
+    cuo::rd_init(&d, buf, len);
+    int k = 0;
+    for (int f = 0; f < frames; f++) {
+        c.VAD_flags[f] = vad[f];
+        int cond = f == 0 ? (cond_first ? cuo::CODE_COND : cuo::CODE_INDEP) : cuo::CODE_COND;
+        cuo::silk_decode_indices(&c, &d, f, 0, cond, &w.sw);
+        cuo::silk_decode_pulses(&d, w.pulses, c.indices.signalType, c.indices.quantOffsetType, c.frame_length,
+                                &w.sw);
+        const cuo::SilkIndices *ix = &c.indices;
+        out[k++] = ix->signalType;
+        out[k++] = ix->quantOffsetType;
+        for (int i = 0; i < 4; i++) out[k++] = ix->GainsIndices[i];
+        for (int i = 0; i < 4; i++) out[k++] = ix->LTPIndex[i];
+        for (int i = 0; i < 17; i++) out[k++] = ix->NLSFIndices[i];
+        out[k++] = ix->lagIndex;
+        out[k++] = ix->contourIndex;
+        out[k++] = ix->NLSFInterpCoef_Q2;
+        out[k++] = ix->PERIndex;
+        out[k++] = ix->LTP_scaleIndex;
+        out[k++] = ix->Seed;
+        for (int i = 0; i < c.frame_length; i++) out[k++] = w.pulses[i];
+    }
+    tail[0] = (uint32_t)cuo::rd_tell(&d);
+    tail[1] = d.rng;
+    return k;
+}
+
 void hc_ec_schedule(const uint8_t *buf, uint32_t len, uint32_t *out)
 {
     static const uint8_t icdf_tab[8] = {120, 112, 96, 64, 32, 16, 8, 0};

@@ -464,3 +464,47 @@ int oref_energy(const uint8_t *buf, uint32_t len, int start, int end, int intra,
     tail[1] = dec.rng;
     return 0;
 }
+
+#include "main.h"
+
+/* SILK entropy decoding of `frames` frames of one channel (silk/decode_indices.c,
+ * decode_pulses.c) at fs_kHz with nb_subfr subframes, from a fresh decoder
+ * state: vad[f] is each frame's VAD flag, the first frame coded independently
+ * (cond_first = 0) or not.  Per frame out receives 33 index words (signalType,
+ * quantOffsetType, GainsIndices[4], LTPIndex[4], NLSFIndices[17], lagIndex,
+ * contourIndex, NLSFInterpCoef_Q2, PERIndex, LTP_scaleIndex, Seed) and then
+ * frame_length pulses; tail receives tell and rng.  Returns words written. */
+int oref_silk_entropy(const uint8_t *buf, uint32_t len, int fs_kHz, int nb_subfr, int frames, const int *vad,
+                      int cond_first, int32_t *out, uint32_t *tail)
+{
+    silk_decoder_state S;
+    ec_dec dec;
+    opus_int16 pulses[MAX_FRAME_LENGTH + SHELL_CODEC_FRAME_LENGTH];
+    silk_init_decoder(&S);
+    S.nb_subfr = nb_subfr;
+    silk_decoder_set_fs(&S, fs_kHz, 48000);
+    ec_dec_init(&dec, (unsigned char *)buf, len);
+    int k = 0;
+    for (int f = 0; f < frames; f++) {
+        S.VAD_flags[f] = vad[f];
+        silk_decode_indices(&S, &dec, f, 0, f == 0 ? (cond_first ? CODE_CONDITIONALLY : CODE_INDEPENDENTLY)
+                                                    : CODE_CONDITIONALLY);
+        silk_decode_pulses(&dec, pulses, S.indices.signalType, S.indices.quantOffsetType, S.frame_length);
+        const SideInfoIndices *ix = &S.indices;
+        out[k++] = ix->signalType;
+        out[k++] = ix->quantOffsetType;
+        for (int i = 0; i < 4; i++) out[k++] = ix->GainsIndices[i];
+        for (int i = 0; i < 4; i++) out[k++] = ix->LTPIndex[i];
+        for (int i = 0; i < 17; i++) out[k++] = ix->NLSFIndices[i];
+        out[k++] = ix->lagIndex;
+        out[k++] = ix->contourIndex;
+        out[k++] = ix->NLSFInterpCoef_Q2;
+        out[k++] = ix->PERIndex;
+        out[k++] = ix->LTP_scaleIndex;
+        out[k++] = ix->Seed;
+        for (int i = 0; i < S.frame_length; i++) out[k++] = pulses[i];
+    }
+    tail[0] = (uint32_t)ec_tell(&dec);
+    tail[1] = dec.rng;
+    return k;
+}

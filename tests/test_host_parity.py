@@ -602,3 +602,31 @@ def test_celt_energy_decoding_matches_libopus(hc):
             res.append((e, tail))
         assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1]), \
             (trial, start, end, C, LM, intra)
+
+
+def test_silk_entropy_decoding_matches_libopus(hc):
+    """SILK side information and excitation pulses (silk/decode_indices.c,
+    decode_pulses.c with the shell coder and signs): every internal rate,
+    10 and 20 ms frames, up to three frames per packet, voiced / unvoiced VAD
+    flags, independent and conditional coding of the first frame, on random
+    bytes.  Every index, every pulse and the range decoder's state equal."""
+    lib = corpus.ref_lib()
+    rng = np.random.default_rng(47)
+    for trial in range(1500):
+        fs = int(rng.choice([8, 12, 16]))
+        nb_subfr = int(rng.choice([2, 4]))
+        frames = 1 if nb_subfr == 2 else int(rng.integers(1, 4))
+        vad = np.ascontiguousarray(rng.integers(0, 2, 3).astype(np.int32))
+        cond = int(rng.integers(0, 2))
+        nbytes = int(rng.integers(10, 250))
+        buf = (ctypes.c_ubyte * nbytes)(*rng.integers(0, 256, nbytes).tolist())
+        res = []
+        for f in (lib.oref_silk_entropy, hc.hc_silk_entropy):
+            out = np.zeros(3 * (33 + 320), np.int32)
+            tail = np.zeros(2, np.uint32)
+            n = f(buf, nbytes, fs, nb_subfr, frames, vad.ctypes.data_as(ctypes.c_void_p), cond,
+                  out.ctypes.data_as(ctypes.c_void_p), tail.ctypes.data_as(ctypes.c_void_p))
+            res.append((n, out, tail))
+        assert res[0][0] == res[1][0] > 0
+        assert np.array_equal(res[0][1], res[1][1]) and np.array_equal(res[0][2], res[1][2]), \
+            (trial, fs, nb_subfr, frames, cond)
