@@ -273,6 +273,33 @@ int hc_silk_entropy(const uint8_t *buf, uint32_t len, int fs_kHz, int nb_subfr, 
     return k;
 }
 
+// The decoder's SILK frames at the internal rate, the oracle's
+// oref_silk_frames layout.
+int hc_silk_frames(const uint8_t *buf, uint32_t len, int fs_kHz, int nb_subfr, int frames, const int32_t *vad,
+                   const int32_t *lost, int16_t *out, uint32_t *tail)
+{
+    static thread_local cuo::SilkChan c;
+    static thread_local cuo::SilkScratch w;
+    cuo::Lanes L{0, 1, 1u};
+    cuo::silk_reset_chan(&c);
+    c.nb_subfr = nb_subfr;
+    c.nFramesPerPacket = 1;
+    cuo::silk_decoder_set_fs(&c, fs_kHz, 48000);
+    cuo::RangeDec d;
+    cuo::rd_init(&d, buf, len);
+    int o = 0;
+    for (int f = 0; f < frames; f++) {
+        int n = 0;
+        c.nFramesDecoded = 0;
+        c.VAD_flags[0] = vad[f];
+        cuo::silk_decode_frame(L, &c, &d, out + o, &n, lost[f], f == 0 ? cuo::CODE_INDEP : cuo::CODE_COND, &w);
+        o += n;
+    }
+    tail[0] = (uint32_t)cuo::rd_tell(&d);
+    tail[1] = d.rng;
+    return o;
+}
+
 void hc_ec_schedule(const uint8_t *buf, uint32_t len, uint32_t *out)
 {
     static const uint8_t icdf_tab[8] = {120, 112, 96, 64, 32, 16, 8, 0};

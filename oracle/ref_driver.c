@@ -508,3 +508,32 @@ int oref_silk_entropy(const uint8_t *buf, uint32_t len, int fs_kHz, int nb_subfr
     tail[1] = dec.rng;
     return k;
 }
+
+/* SILK frames at the internal rate (silk/decode_frame.c: indices, pulses,
+ * parameters, excitation, LTP / LPC synthesis, PLC and CNG) of one channel,
+ * one frame per packet, the decoder state carried from frame to frame, all
+ * bits from one range decoder: lost[f] conceals frame f, vad[f] is its VAD
+ * flag.  out receives the frames back to back; tail tell and rng.  Returns
+ * samples written. */
+int oref_silk_frames(const uint8_t *buf, uint32_t len, int fs_kHz, int nb_subfr, int frames, const int *vad,
+                     const int *lost, int16_t *out, uint32_t *tail)
+{
+    silk_decoder_state S;
+    ec_dec dec;
+    silk_init_decoder(&S);
+    S.nb_subfr = nb_subfr;
+    S.nFramesPerPacket = 1;
+    silk_decoder_set_fs(&S, fs_kHz, 48000);
+    ec_dec_init(&dec, (unsigned char *)buf, len);
+    int o = 0;
+    for (int f = 0; f < frames; f++) {
+        opus_int32 n = 0;
+        S.nFramesDecoded = 0;
+        S.VAD_flags[0] = vad[f];
+        silk_decode_frame(&S, &dec, out + o, &n, lost[f], f == 0 ? CODE_INDEPENDENTLY : CODE_CONDITIONALLY, 0);
+        o += n;
+    }
+    tail[0] = (uint32_t)ec_tell(&dec);
+    tail[1] = dec.rng;
+    return o;
+}

@@ -630,3 +630,33 @@ def test_silk_entropy_decoding_matches_libopus(hc):
         assert res[0][0] == res[1][0] > 0
         assert np.array_equal(res[0][1], res[1][1]) and np.array_equal(res[0][2], res[1][2]), \
             (trial, fs, nb_subfr, frames, cond)
+
+
+def test_silk_frames_match_libopus(hc):
+    """Whole SILK frames at the internal rate (silk/decode_frame.c: indices,
+    pulses, NLSF / LPC / pitch / LTP parameters, excitation, LTP and LPC
+    synthesis, concealment of lost frames, comfort noise), state carried over
+    eight frames decoded from random bytes, every rate and frame length.
+    Every sample and the range decoder's state equal."""
+    lib = corpus.ref_lib()
+    rng = np.random.default_rng(53)
+    for trial in range(400):
+        fs = int(rng.choice([8, 12, 16]))
+        nb_subfr = int(rng.choice([2, 4]))
+        frames = 8
+        vad = np.ascontiguousarray(rng.integers(0, 2, frames).astype(np.int32))
+        lost = np.ascontiguousarray((rng.random(frames) < 0.15).astype(np.int32))
+        lost[0] = 0
+        nbytes = int(rng.integers(40, 600))
+        buf = (ctypes.c_ubyte * nbytes)(*rng.integers(0, 256, nbytes).tolist())
+        res = []
+        for f in (lib.oref_silk_frames, hc.hc_silk_frames):
+            out = np.zeros(frames * 320, np.int16)
+            tail = np.zeros(2, np.uint32)
+            n = f(buf, nbytes, fs, nb_subfr, frames, vad.ctypes.data_as(ctypes.c_void_p),
+                  lost.ctypes.data_as(ctypes.c_void_p), out.ctypes.data_as(ctypes.c_void_p),
+                  tail.ctypes.data_as(ctypes.c_void_p))
+            res.append((n, out, tail))
+        assert res[0][0] == res[1][0] == frames * nb_subfr * 5 * fs
+        assert np.array_equal(res[0][1], res[1][1]) and np.array_equal(res[0][2], res[1][2]), \
+            (trial, fs, nb_subfr, vad, lost)
