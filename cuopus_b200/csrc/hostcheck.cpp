@@ -300,6 +300,27 @@ int hc_silk_frames(const uint8_t *buf, uint32_t len, int fs_kHz, int nb_subfr, i
     return o;
 }
 
+// The decoder's CELT frames of one stream, the oracle's oref_celt_frames
+// layout (its final range is the state's rng after each frame).
+int hc_celt_frames(const uint8_t *data, const uint32_t *lens, int frames, int C, int LM, int end, int16_t *out,
+                   uint32_t *rng)
+{
+    static thread_local cuo::CeltDec st;
+    static thread_local cuo::CeltScratch w;
+    cuo::Lanes L{0, 1, 1u};
+    cuo::celt_init(&st, C);
+    st.end = end;
+    int N = 120 << LM;
+    size_t off = 0;
+    for (int f = 0; f < frames; f++) {
+        int ret = cuo::celt_decode(L, &st, lens[f] ? data + off : nullptr, (int)lens[f], out + (size_t)f * N * C, N,
+                                   nullptr, 0, &w);
+        rng[f] = ret < 0 ? (uint32_t)ret : st.rng;
+        off += lens[f];
+    }
+    return 0;
+}
+
 void hc_ec_schedule(const uint8_t *buf, uint32_t len, uint32_t *out)
 {
     static const uint8_t icdf_tab[8] = {120, 112, 96, 64, 32, 16, 8, 0};

@@ -537,3 +537,31 @@ int oref_silk_frames(const uint8_t *buf, uint32_t len, int fs_kHz, int nb_subfr,
     tail[1] = dec.rng;
     return o;
 }
+
+/* CELT frames (celt/celt_decoder.c celt_decode_with_ec: energies, allocation,
+ * band shapes, anti-collapse, synthesis, post-filter, deemphasis, and the
+ * concealment for lost frames) of one stream from a fresh 48 kHz decoder with
+ * signalling off and end band `end`: frame f is lens[f] bytes of data (0 =
+ * lost), 120 << LM samples per channel into out; rng[f] receives the final
+ * range, or the error code when the decode fails.  Returns 0. */
+int oref_celt_frames(const uint8_t *data, const uint32_t *lens, int frames, int C, int LM, int end, int16_t *out,
+                     uint32_t *rng)
+{
+    CELTDecoder *st = (CELTDecoder *)malloc((size_t)celt_decoder_get_size(C));
+    if (!st) return -1;
+    celt_decoder_init(st, 48000, C);
+    opus_custom_decoder_ctl(st, CELT_SET_SIGNALLING(0));
+    opus_custom_decoder_ctl(st, CELT_SET_END_BAND(end));
+    int N = 120 << LM;
+    size_t off = 0;
+    for (int f = 0; f < frames; f++) {
+        int ret = celt_decode_with_ec(st, lens[f] ? data + off : NULL, (int)lens[f], out + (size_t)f * N * C, N,
+                                      NULL, 0);
+        opus_uint32 r = 0;
+        opus_custom_decoder_ctl(st, OPUS_GET_FINAL_RANGE(&r));
+        rng[f] = ret < 0 ? (uint32_t)ret : r;
+        off += lens[f];
+    }
+    free(st);
+    return 0;
+}

@@ -660,3 +660,30 @@ def test_silk_frames_match_libopus(hc):
         assert res[0][0] == res[1][0] == frames * nb_subfr * 5 * fs
         assert np.array_equal(res[0][1], res[1][1]) and np.array_equal(res[0][2], res[1][2]), \
             (trial, fs, nb_subfr, vad, lost)
+
+
+def test_celt_frames_match_libopus(hc):
+    """Whole CELT frames (celt/celt_decoder.c celt_decode_with_ec from a fresh
+    decoder: energies, allocation, band shapes, anti-collapse, IMDCT, post
+    filter, deemphasis, and the concealment of lost frames), ten frames of
+    random bytes per stream with the state carried over, every frame size,
+    mono and stereo, every end band.  Every sample and final range equal."""
+    lib = corpus.ref_lib()
+    rng = np.random.default_rng(59)
+    for trial in range(300):
+        C, LM = 1 + int(rng.integers(0, 2)), int(rng.integers(0, 4))
+        end = int(rng.choice([13, 17, 19, 21]))
+        frames = 10
+        lens = rng.integers(2, 160, frames).astype(np.uint32)
+        lens[rng.random(frames) < 0.12] = 0
+        lens[0] = max(int(lens[0]), 2)
+        data = rng.integers(0, 256, int(lens.sum()) + 1).astype(np.uint8)
+        res = []
+        for f in (lib.oref_celt_frames, hc.hc_celt_frames):
+            out = np.zeros(frames * (120 << LM) * C, np.int16)
+            fr = np.zeros(frames, np.uint32)
+            f(data.ctypes.data_as(ctypes.c_void_p), lens.ctypes.data_as(ctypes.c_void_p), frames, C, LM, end,
+              out.ctypes.data_as(ctypes.c_void_p), fr.ctypes.data_as(ctypes.c_void_p))
+            res.append((out, fr))
+        assert np.array_equal(res[0][1], res[1][1]), (trial, C, LM, end, lens)
+        assert np.array_equal(res[0][0], res[1][0]), (trial, C, LM, end, lens)
