@@ -6,7 +6,7 @@ bytes (mode, frame sizes, bandwidth, channels, sizes) by an FP32 MLP
 16 -> 64 -> 64 -> 1 with ReLU, trained on the GPU on log cycle counts that the
 decoder itself records per chain (res[c].time_us).  The queue schedule then
 visits chains longest first by prediction.  The fallback, and the baseline the
-model is judged against, is the packet-count order (packets x channels).
+model is measured against, is the packet-count order (packets x channels).
 
 The model only orders the work; decoded samples never depend on it.
 """

@@ -111,7 +111,7 @@ def test_gpu_forward_and_gradient_match_oracle(cuda):
 @pytest.mark.gpu
 def test_gpu_training_learns_decode_cost_and_beats_packet_order(cuda):
     """Record per-chain decode cycles on a mixed batch, train on half, and
-    judge on the other half against the fallback (packets x channels, fitted
+    evaluate on the other half against the fallback (packets x channels, fitted
     to log cycles by least squares on the same half):
       * the network explains more of the variance of log cycles;
       * predicting the makespan of a longest-first schedule from the predicted
