@@ -321,6 +321,34 @@ int hc_celt_frames(const uint8_t *data, const uint32_t *lens, int frames, int C,
     return 0;
 }
 
+// The decoder's fixed-point helpers elementwise, numbered as the oracle's
+// oref_mathops.
+int hc_mathops(int op, const int32_t *a, const int32_t *b, const int32_t *q, int n, int32_t *out)
+{
+    for (int i = 0; i < n; i++) {
+        int32_t r;
+        switch (op) {
+        case 0: r = (int32_t)cuo::c_isqrt32((uint32_t)a[i]); break;
+        case 1: r = cuo::c_rcp(a[i]); break;
+        case 2: r = cuo::c_frac_div32(a[i], b[i]); break;
+        case 3: r = cuo::c_rsqrt_norm(a[i]); break;
+        case 4: r = cuo::c_sqrt(a[i]); break;
+        case 5: r = cuo::c_cos_norm(a[i]); break;
+        case 6: r = cuo::c_exp2((int16_t)a[i]); break;
+        case 7: r = cuo::bitexact_cos((int16_t)a[i]); break;
+        case 8: r = cuo::bitexact_log2tan(a[i], b[i]); break;
+        case 9: r = cuo::s_sqrt_approx(a[i]); break;
+        case 10: r = cuo::s_div32_varq(a[i], b[i], q[i]); break;
+        case 11: r = cuo::s_inverse32_varq(a[i], q[i]); break;
+        case 12: r = cuo::s_log2lin(a[i]); break;
+        case 13: r = cuo::s_lin2log(a[i]); break;
+        default: return -1;
+        }
+        out[i] = r;
+    }
+    return 0;
+}
+
 void hc_ec_schedule(const uint8_t *buf, uint32_t len, uint32_t *out)
 {
     static const uint8_t icdf_tab[8] = {120, 112, 96, 64, 32, 16, 8, 0};

@@ -565,3 +565,37 @@ int oref_celt_frames(const uint8_t *data, const uint32_t *lens, int frames, int 
     free(st);
     return 0;
 }
+
+/* Fixed-point helpers evaluated elementwise over arrays, for the decoder's
+ * restatements of them: op 0 isqrt32, 1 celt_rcp, 2 frac_div32(a, b),
+ * 3 celt_rsqrt_norm, 4 celt_sqrt, 5 celt_cos_norm, 6 celt_exp2 (celt/mathops.c,
+ * celt/mathops.h), 7 bitexact_cos, 8 bitexact_log2tan(a, b) (celt/bands.c:68-90),
+ * 9 silk_SQRT_APPROX, 10 silk_DIV32_varQ(a, b, q), 11 silk_INVERSE32_varQ(a, q)
+ * (silk/Inlines.h:71-166), 12 silk_log2lin (silk/log2lin.c), 13 silk_lin2log
+ * (silk/lin2log.c).  Returns -1 for an unknown op. */
+#include "mathops.h"
+int oref_mathops(int op, const int32_t *a, const int32_t *b, const int32_t *q, int n, int32_t *out)
+{
+    for (int i = 0; i < n; i++) {
+        int32_t r;
+        switch (op) {
+        case 0: r = (int32_t)isqrt32((opus_uint32)a[i]); break;
+        case 1: r = celt_rcp(a[i]); break;
+        case 2: r = frac_div32(a[i], b[i]); break;
+        case 3: r = celt_rsqrt_norm(a[i]); break;
+        case 4: r = celt_sqrt(a[i]); break;
+        case 5: r = celt_cos_norm(a[i]); break;
+        case 6: r = celt_exp2((opus_val16)a[i]); break;
+        case 7: r = bitexact_cos((opus_int16)a[i]); break;
+        case 8: r = bitexact_log2tan(a[i], b[i]); break;
+        case 9: r = silk_SQRT_APPROX(a[i]); break;
+        case 10: r = silk_DIV32_varQ(a[i], b[i], q[i]); break;
+        case 11: r = silk_INVERSE32_varQ(a[i], q[i]); break;
+        case 12: r = silk_log2lin(a[i]); break;
+        case 13: r = silk_lin2log(a[i]); break;
+        default: return -1;
+        }
+        out[i] = r;
+    }
+    return 0;
+}

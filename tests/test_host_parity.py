@@ -687,3 +687,72 @@ def test_celt_frames_match_libopus(hc):
             res.append((out, fr))
         assert np.array_equal(res[0][1], res[1][1]), (trial, C, LM, end, lens)
         assert np.array_equal(res[0][0], res[1][0]), (trial, C, LM, end, lens)
+
+
+def _mathops_cases(rng):
+    """(op, a, b, q) arrays over each helper's input domain: exhaustive where it
+    is 16-bit or a short range, random draws plus the ends elsewhere."""
+    i32 = lambda x: np.asarray(x, np.int64).astype(np.int32)
+    rnd = lambda lo, hi, n: rng.integers(lo, hi, n, dtype=np.int64)
+    pos = np.concatenate([np.arange(1, 1 << 17), rnd(1, 1 << 31, 1 << 17), [2**31 - 1]])
+    cases = []
+    cases.append((0, i32(np.concatenate([np.arange(1, 1 << 17), rnd(1, 1 << 32, 1 << 17), [2**32 - 1]]))))
+    cases.append((1, i32(pos)))
+    b = rnd(1, 1 << 31, 1 << 17)
+    a = (rng.random(len(b)) * 2 - 1) * b
+    cases.append((2, i32(a), i32(b)))
+    cases.append((3, i32(np.arange(16384, 65536))))
+    cases.append((4, i32(np.concatenate([[0], pos]))))
+    cases.append((5, i32(np.arange(-(1 << 18), (1 << 18) + 1))))
+    cases.append((6, i32(np.arange(-32768, 32768))))
+    cases.append((7, i32(np.arange(-32768, 32768))))
+    cases.append((8,))              # bitexact_log2tan: built from bitexact_cos in the test
+    sgn = np.concatenate([pos, -pos[::7], [0]])
+    cases.append((9, i32(sgn)))
+    a = rnd(-(2**31 - 1), 2**31, 1 << 17)
+    b = rnd(1, 2**31, 1 << 17) * rng.choice([-1, 1], 1 << 17)
+    cases.append((10, i32(a), i32(b), i32(rnd(0, 31, 1 << 17))))
+    cases.append((11, i32(b), None, i32(rnd(1, 62, 1 << 17))))
+    cases.append((12, i32(np.arange(-256, 4300))))
+    cases.append((13, i32(np.concatenate([np.arange(0, 1 << 17), rnd(1, 2**31, 1 << 17)]))))
+    return cases, np.arange(0, 16385)
+
+
+def test_fixed_point_helpers_match_libopus(hc):
+    """The decoder's fixed-point helpers against libopus's own, elementwise over
+    their input domains (celt/mathops.c isqrt32, celt_rcp, frac_div32,
+    celt_rsqrt_norm, celt_sqrt, celt_cos_norm; celt/mathops.h celt_exp2;
+    celt/bands.c:68-90 bitexact_cos, bitexact_log2tan; silk/Inlines.h:71-166
+    silk_SQRT_APPROX, silk_DIV32_varQ, silk_INVERSE32_varQ; silk/log2lin.c,
+    silk/lin2log.c).  Every output word equal."""
+    lib = corpus.ref_lib()
+    rng = np.random.default_rng(61)
+    cases, theta = _mathops_cases(rng)
+
+    def run(f, op, a, b=None, q=None):
+        n = len(a)
+        b = np.zeros(n, np.int32) if b is None else b
+        q = np.zeros(n, np.int32) if q is None else q
+        out = np.zeros(n, np.int32)
+        vp = lambda x: x.ctypes.data_as(ctypes.c_void_p)
+        assert f(op, vp(a), vp(b), vp(q), n, vp(out)) == 0
+        return out
+
+    for case in cases:
+        op = case[0]
+        if op == 8:
+            # the decoder's own domain: the sine / cosine of every split angle
+            c = run(lib.oref_mathops, 7, theta.astype(np.int32))
+            s = run(lib.oref_mathops, 7, (16384 - theta).astype(np.int32))
+            r1 = rng.integers(1, 32768, 1 << 16).astype(np.int32)
+            r2 = rng.integers(1, 32768, 1 << 16).astype(np.int32)
+            a, b, q = np.concatenate([s, r1]), np.concatenate([c, r2]), None
+        else:
+            a = case[1]
+            b = case[2] if len(case) > 2 else None
+            q = case[3] if len(case) > 3 else None
+        want = run(lib.oref_mathops, op, a, b, q)
+        got = run(hc.hc_mathops, op, a, b, q)
+        bad = np.flatnonzero(want != got)
+        assert bad.size == 0, (op, int(a[bad[0]]), None if b is None else int(b[bad[0]]), int(want[bad[0]]),
+                               int(got[bad[0]]))
