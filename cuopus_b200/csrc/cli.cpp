@@ -36,6 +36,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <sys/socket.h>
+#include <sys/time.h>
 #include <sys/un.h>
 #include <time.h>
 #include <unistd.h>
@@ -440,13 +441,17 @@ int run_serve(const char *sock_path)
     int idle_s = 600;
     const char *e = getenv("CUOPUS_SERVE_IDLE_S");
     if (e && atoi(e) > 0) idle_s = atoi(e);
+    struct sockaddr_un addr;
+    if (strlen(sock_path) >= sizeof(addr.sun_path)) {
+        fprintf(stderr, "cuopus_decode: socket path longer than %zu bytes\n", sizeof(addr.sun_path) - 1);
+        return 2;
+    }
     unlink(sock_path);
     int srv = socket(AF_UNIX, SOCK_STREAM, 0);
     if (srv < 0) {
         perror("socket");
         return 2;
     }
-    struct sockaddr_un addr;
     memset(&addr, 0, sizeof addr);
     addr.sun_family = AF_UNIX;
     strncpy(addr.sun_path, sock_path, sizeof(addr.sun_path) - 1);
@@ -479,6 +484,10 @@ int run_serve(const char *sock_path)
         }
         int fd = accept(srv, nullptr, nullptr);
         if (fd < 0) continue;
+        // A client that connects and sends no request line must not hold the
+        // single-threaded loop: its read gives up after 30 s.
+        struct timeval rto = {30, 0};
+        setsockopt(fd, SOL_SOCKET, SO_RCVTIMEO, &rto, sizeof rto);
         size_t got = 0;
         while (got < line.size() - 1) {
             ssize_t r = read(fd, line.data() + got, line.size() - 1 - got);

@@ -61,6 +61,33 @@ def test_bad_file(cli, tmp_path):
     assert r.returncode == 1
 
 
+def test_daemon_protocol_without_decoding(cli):
+    """The daemon's request handling that needs no device: PING, a request for
+    a missing file, an unknown command and QUIT, and the refusal of a socket
+    path that does not fit sockaddr_un."""
+    d = tempfile.mkdtemp()
+    r = subprocess.run([cli, "--serve", os.path.join(d, "x" * 200)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2 and "socket path" in r.stderr
+    sock = os.path.join(d, "s")
+    env = dict(os.environ, CUOPUS_SERVE_IDLE_S="60")
+    p = subprocess.Popen([cli, "--serve", sock], env=env, stderr=subprocess.PIPE, text=True)
+    try:
+        t0 = time.time()
+        while not os.path.exists(sock) and time.time() - t0 < 60:
+            time.sleep(0.1)
+        time.sleep(0.2)
+        assert _ask(sock, "PING") == "PONG 2"
+        assert _ask(sock, "DECODE 1 250 32 /nonexistent %s" % os.path.join(d, "o")).startswith("ERR")
+        assert _ask(sock, "DECODE16F 1 250").startswith("ERR bad request")
+        assert _ask(sock, "BOGUS").startswith("ERR")
+        assert _ask(sock, "QUIT") == "BYE"
+        assert p.wait(timeout=30) == 0
+        assert not os.path.exists(sock)
+    finally:
+        if p.poll() is None:
+            p.kill()
+
+
 # ------------------------------------------------------------------ GPU
 
 def _want_i16(name, seg=1.0, pre=250.0):
