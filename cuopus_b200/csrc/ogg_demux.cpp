@@ -145,6 +145,7 @@ bool demux(const uint8_t *data, size_t n, const Options &opt, Demux &d, std::str
         for (size_t i = 0; i < spans.size(); i++) {
             if (i == 0 || spans[i - 1].done) first_span = i;
             acc += spans[i].len;
+            if (acc > 0xFFFFFFFFull) { err = "packet too large"; return false; }
             if (spans[i].done) {
                 pkt_span_first.push_back(first_span);
                 pkt_len.push_back((uint32_t)acc);
@@ -244,6 +245,10 @@ bool build_chains(const Demux &d, double seconds, double preroll_ms, Chains &c, 
     uint32_t npk = d.n_packets();
     if (total <= 0) { err = "no playable samples"; return false; }
     if (step <= 0) { err = "bad segment length"; return false; }
+    // Header pages can carry a granule (hence playable samples) with no audio
+    // packet after them; the reference's cu_build_chains2 then reads past its
+    // prefix-sum array.
+    if (npk == 0) { err = "no audio packets"; return false; }
     std::vector<int64_t> cum(npk + 1, 0);
     for (uint32_t k = 0; k < npk; k++)
         cum[k + 1] = cum[k] + toc_samples48(d.blob.data() + d.off[k], d.len[k]);

@@ -78,18 +78,23 @@ def demux(data: bytes) -> dict:
         pos = body + blen
     if not page_gran:
         raise DemuxError("no OGG pages found")
-    packets, pages = [], []
-    part = b""
+    packets, pages, first_span = [], [], []
+    part, start = b"", None
     for s, e, done, pg in spans:
+        if start is None:
+            start = e - s
         part += data[s:e]
         if done:
             packets.append(part)
             pages.append(pg)
-            part = b""
+            first_span.append(start)
+            part, start = b"", None
     if len(packets) < 2:
         raise DemuxError("not an OGG Opus stream (fewer than 2 packets)")
     head = packets[0]
-    if len(head) < 19 or not head.startswith(b"OpusHead"):
+    # the header fields are read from the packet's first span (a page-split
+    # OpusHead whose first piece is shorter than 12 bytes is refused)
+    if len(head) < 19 or first_span[0] < 12 or not head.startswith(b"OpusHead"):
         raise DemuxError("not an OGG Opus stream (no OpusHead)")
     channels = head[9]
     preskip = head[10] | (head[11] << 8)
@@ -134,6 +139,10 @@ def build_chains(ix: dict, seconds: float, preroll_ms: float):
         raise DemuxError("no playable samples")
     if step <= 0:
         raise DemuxError("bad segment length")
+    if not pk:
+        # header pages may carry a granule with no audio packet after them
+        # (cuopus_demux.h:293-378 reads past its prefix sums here)
+        raise DemuxError("no audio packets")
     cum = [0]
     for p in pk:
         cum.append(cum[-1] + toc_samples48(p))
@@ -147,6 +156,8 @@ def build_chains(ix: dict, seconds: float, preroll_ms: float):
         if cum[first + 1] <= target:
             first += 1
         last = max(bisect.bisect_left(so, te) - 1, first)
+        if first >= len(pk):
+            raise DemuxError("chain %d: packet range beyond the stream" % k)
         trim, keep = ts - so[first], pe - ps
         if trim < 0:
             raise DemuxError("chain %d: negative trim %d" % (k, trim))

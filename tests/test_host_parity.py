@@ -159,6 +159,103 @@ def test_page_crc_check(cn, monkeypatch):
 
 # ------------------------------------------------------------------ host same-source decoder
 
+def _mutate(rng, data):
+    """One seeded damage of an Ogg stream: a truncation, byte flips, a page's
+    granule, lacing value, segment count or presence changed, or the OpusHead
+    channel / preskip bytes rewritten."""
+    b = bytearray(data)
+    pages = [i for i in range(len(b) - 3) if b[i:i + 4] == b"OggS"]
+    pg = pages[int(rng.integers(0, len(pages)))]
+    kind = int(rng.integers(0, 9))
+    if kind == 0:
+        return bytes(b[:int(rng.integers(0, len(b)))])
+    if kind == 1:
+        for i in rng.integers(0, len(b), int(rng.integers(1, 9))):
+            b[i] ^= 1 << int(rng.integers(0, 8))
+    elif kind == 2:
+        g = int.from_bytes(b[pg + 6:pg + 14], "little", signed=True)
+        g = int(rng.choice([-1, 0, g + int(rng.integers(-960, 961)), int(rng.integers(0, 1 << 40))]))
+        b[pg + 6:pg + 14] = g.to_bytes(8, "little", signed=True)
+    elif kind == 3 and b[pg + 26]:
+        b[pg + 27 + int(rng.integers(0, b[pg + 26]))] = int(rng.choice([0, 255, int(rng.integers(0, 256))]))
+    elif kind == 4:
+        b[pg + 26] = int(rng.integers(0, 256))
+    elif kind == 5:
+        nxt = [p for p in pages if p > pg]
+        end = nxt[0] if nxt else len(b)
+        del b[pg:end]
+    elif kind == 6:
+        nxt = [p for p in pages if p > pg]
+        end = nxt[0] if nxt else len(b)
+        b[pg:pg] = b[pg:end]
+    elif kind == 7:
+        h = b.find(b"OpusHead")
+        b[h + 9] = int(rng.integers(0, 4))
+    else:
+        h = b.find(b"OpusHead")
+        b[h + 10:h + 12] = int(rng.integers(0, 65536)).to_bytes(2, "little")
+    return bytes(b)
+
+
+def _port_index(data, seg, pre):
+    try:
+        ix = ogg_port.demux(data)
+        if ix["channels"] not in (1, 2) or ix["granule_match"] != ix["granule_checked"]:
+            return None
+        return ix, ogg_port.build_chains(ix, seg, pre)
+    except ogg_port.DemuxError:
+        return None
+
+
+def test_demuxer_on_damaged_streams_agrees_with_the_port(cn, monkeypatch):
+    """1,500 seeded damages of the golden streams (truncations, bit flips,
+    granules, lacing values, segment counts, dropped and repeated pages,
+    OpusHead channel / preskip bytes): the C++ demuxer and the oracle's port of
+    the reference indexer (ogg_index.py:75-367) refuse the same streams, with
+    rc 1 and nothing else, and give identical packets, lengths and chain tables
+    for the rest."""
+    monkeypatch.delenv("CUOPUS_OGG_CRC", raising=False)
+    monkeypatch.delenv("CUOPUS_GRANULE", raising=False)
+    rng = np.random.default_rng(67)
+    names = sorted(INDEX)
+    accepted = refused = 0
+    for trial in range(1500):
+        data = _mutate(rng, _stream(names[trial % len(names)]))
+        seg, pre = (1.0, 250.0) if trial % 2 else (0.5, 80.0)
+        want = _port_index(data, seg, pre)
+        try:
+            got = cn.index(data, seg_s=seg, preroll_ms=pre)
+        except cn.CuopusError as e:
+            assert e.rc == 1, (trial, e)
+            got = None
+        assert (want is None) == (got is None), (trial, want is None, str(got))
+        if got is None:
+            refused += 1
+            continue
+        accepted += 1
+        ix, chains = want
+        assert got.channels == ix["channels"] and got.play48 == ix["play48"], trial
+        assert [int(v) for v in got.pkt_len] == [len(p) for p in ix["packets"]], trial
+        assert got.blob.tobytes() == b"".join(ix["packets"]), trial
+        assert [tuple(int(v) for v in c) for c in zip(got.first, got.npkts, got.trim, got.keep)] == chains, trial
+    assert accepted > 200 and refused > 200, (accepted, refused)
+
+
+def test_header_only_stream_with_a_granule_is_refused(cn):
+    """Two header packets and no audio, the header page carrying a granule past
+    the preskip: playable samples without packets.  Refused with rc 1 (the
+    reference's chain builder reads past its prefix sums here)."""
+    data = bytearray(_stream("plain_a"))
+    pages = [i for i in range(len(data) - 3) if data[i:i + 4] == b"OggS"]
+    head = data[:pages[2]]                       # OpusHead page + OpusTags page
+    head[6:14] = (100000).to_bytes(8, "little")
+    with pytest.raises(ogg_port.DemuxError):
+        _ = ogg_port.build_chains(ogg_port.demux(bytes(head)), 1.0, 250.0)
+    with pytest.raises(cn.CuopusError) as e:
+        cn.index(bytes(head))
+    assert e.value.rc == 1 and "no audio packets" in str(e.value)
+
+
 def test_range_decoder_gate_schedules(hc):
     with open(os.path.join(GOLD, "rangedec.json")) as f:
         cases = json.load(f)
