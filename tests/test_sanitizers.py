@@ -1,10 +1,12 @@
-"""The decoder sources under UndefinedBehaviorSanitizer (CPU only).
+"""The decoder and demuxer sources under the sanitizers (CPU only).
 
 The host same-source build (one lane per chain) is compiled again with
 -fsanitize=undefined and aborts on the first report; it must decode mixed
 SILK / hybrid / CELT streams, mono and stereo, with lost packets, DTX frames
 and in-band FEC, to libopus's samples.  Integer overflow in a signed type, an
-out-of-range shift or a misaligned access anywhere in the decoder fails it."""
+out-of-range shift or a misaligned access anywhere in the decoder fails it.
+The host demuxer is built with AddressSanitizer as well and parses damaged
+streams (tests/asan_demux_driver.cpp)."""
 import ctypes
 import os
 import shutil
@@ -86,3 +88,54 @@ def test_decoder_has_no_undefined_behaviour(hc_ubsan):
 if __name__ == "__main__":
     import sys
     _decode_all(sys.argv[1])
+
+
+def test_demuxer_on_damaged_streams_under_address_sanitizer(tmp_path):
+    """The host demuxer and chain builder (ogg_demux.cpp) built with
+    AddressSanitizer + UndefinedBehaviorSanitizer and run over 1,500 seeded
+    damages of the golden streams, each in a heap buffer of exactly its size,
+    under the default options, the page-CRC check and the granule
+    warn-and-resync policy: no report, and under the default options the same
+    streams accepted as by the oracle's port, with the same lengths."""
+    import json
+    import struct
+    import sys
+    if not shutil.which("g++"):
+        pytest.skip("g++ is not installed")
+    exe = str(tmp_path / "asan_demux")
+    r = subprocess.run(["g++", "-O1", "-g", "-std=c++17", "-w", "-fsanitize=address,undefined",
+                        "-fno-sanitize-recover=all", "-I", CSRC, os.path.join(CSRC, "ogg_demux.cpp"),
+                        os.path.join(ROOT, "tests", "asan_demux_driver.cpp"), "-o", exe],
+                       capture_output=True, text=True)
+    if r.returncode != 0 and "asan" in (r.stderr + r.stdout).lower():
+        pytest.skip("ASan runtime unavailable: " + r.stderr[-200:])
+    assert r.returncode == 0, r.stderr[-2000:]
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from test_host_parity import _mutate, _port_index
+    gold = os.path.join(ROOT, "tests", "golden")
+    names = sorted(json.load(open(os.path.join(gold, "index.json"))))
+    streams = {n: open(os.path.join(gold, "streams", n + ".opus"), "rb").read() for n in names}
+    rng = np.random.default_rng(71)
+    recs = [_mutate(rng, streams[names[i % len(names)]]) for i in range(1500)]
+    recs += list(streams.values())
+    path = tmp_path / "records"
+    path.write_bytes(b"".join(struct.pack("<I", len(d)) + d for d in recs))
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=1:abort_on_error=0",
+               UBSAN_OPTIONS="print_stacktrace=1:halt_on_error=1")
+    p = subprocess.run([exe, str(path)], capture_output=True, text=True, env=env, timeout=600)
+    assert p.returncode == 0, p.stderr[-4000:]
+    lines = p.stdout.splitlines()
+    assert len(lines) == 3 * len(recs)
+    accepted = 0
+    for i, d in enumerate(recs):
+        seg, pre = (1.0, 250.0) if i % 2 else (0.5, 80.0)
+        want = _port_index(d, seg, pre)
+        got = lines[3 * i].split()
+        if want is None:
+            assert got == ["refused"], i
+            continue
+        accepted += 1
+        ix, chains = want
+        assert got == ["ok", str(ix["play48"]), str(ix["channels"]), str(len(ix["packets"])), str(len(chains)),
+                       str(sum(c[3] for c in chains))], i
+    assert accepted > 200
