@@ -1,10 +1,12 @@
 """The decoder and demuxer sources under the sanitizers (CPU only).
 
 The host same-source build (one lane per chain) is compiled again with
--fsanitize=undefined and aborts on the first report; it must decode mixed
+-fsanitize=address,undefined (UBSan alone where g++ has no ASan runtime) and
+aborts on the first report; it must decode mixed
 SILK / hybrid / CELT streams, mono and stereo, with lost packets, DTX frames
-and in-band FEC, to libopus's samples.  Integer overflow in a signed type, an
-out-of-range shift or a misaligned access anywhere in the decoder fails it.
+and in-band FEC, and chains ending in random packets, to libopus's samples.
+Integer overflow in a signed type, an out-of-range shift, a misaligned access
+or a read or write out of bounds anywhere in the decoder fails it.
 The host demuxer is built with AddressSanitizer as well and parses damaged
 streams (tests/asan_demux_driver.cpp)."""
 import ctypes
@@ -35,22 +37,34 @@ def _lossy(packets, seed, p_lost, p_dtx):
     return out
 
 
+def _asan_runtime():
+    """Path of g++'s AddressSanitizer runtime, or None.  A sanitised shared
+    library loaded into Python needs it preloaded."""
+    r = subprocess.run(["g++", "-print-file-name=libasan.so"], capture_output=True, text=True)
+    path = r.stdout.strip()
+    return path if os.path.isabs(path) and os.path.exists(path) else None
+
+
 @pytest.fixture(scope="module")
 def hc_ubsan(tmp_path_factory):
+    """(library, LD_PRELOAD value): the host build under UBSan, and under
+    AddressSanitizer too where g++ has its runtime."""
     if not shutil.which("g++"):
         pytest.skip("g++ is not installed")
     try:
         corpus.ref_lib()
     except OSError as e:
         pytest.skip(str(e))
+    asan = _asan_runtime()
     out = str(tmp_path_factory.mktemp("ubsan") / "libhc_ubsan.so")
-    r = subprocess.run(["g++", "-O1", "-std=c++17", "-fPIC", "-shared", "-w", "-fsanitize=undefined",
+    r = subprocess.run(["g++", "-O1", "-std=c++17", "-fPIC", "-shared", "-w",
+                        "-fsanitize=address,undefined" if asan else "-fsanitize=undefined",
                         "-fno-sanitize-recover=all", "-I", CSRC, os.path.join(CSRC, "hostcheck.cpp"), "-o", out,
                         "-lpthread"], capture_output=True, text=True)
     if r.returncode != 0 and "ubsan" in (r.stderr + r.stdout).lower():
         pytest.skip("UBSan runtime unavailable: " + r.stderr[-200:])
     assert r.returncode == 0, r.stderr[-2000:]
-    return out
+    return out, asan
 
 
 def _decode_all(lib_path):
@@ -72,22 +86,38 @@ def _decode_all(lib_path):
             assert stop == int(ref["status"][0])
             assert np.array_equal(ns, ref["nsamp"][0]) and np.array_equal(rg, ref["rng"][0])
             assert np.array_equal(pcm, ref["pcm"][0]), (seed, fec)
+    # random packets (any TOC, framing code, padding and payload) after up to
+    # three good ones: the decoder's status, counts and samples are libopus's
+    rng = np.random.default_rng(79)
+    for channels in (1, 2):
+        good = ogg_port.demux(corpus.make_stream(dict(kind="mixed", seed=78100, seconds=1.0,
+                                                      channels=channels)))["packets"]
+        pk, chains = [], []
+        for k in range(200):
+            n_good = int(rng.integers(0, 4))
+            chains.append((len(pk), n_good + 1))
+            pk += good[:n_good]
+            pk.append(rng.integers(0, 256, int(rng.integers(1, 400)), dtype=np.uint8).tobytes())
+        ref = ref_decode.decode_chains(pk, chains, channels)
+        got = host_decode(hc, pk, chains, channels)
+        for c, (pcm, ns, rg, stop, _) in enumerate(got):
+            assert stop == int(ref["status"][c]), (channels, c)
+            assert np.array_equal(ns, ref["nsamp"][c]) and np.array_equal(rg, ref["rng"][c]), (channels, c)
+            assert np.array_equal(pcm, ref["pcm"][c]), (channels, c)
 
 
 def test_decoder_has_no_undefined_behaviour(hc_ubsan):
     """Run in a child process, so that a sanitizer report (which aborts) fails
     this test with the report instead of ending the test run."""
     import sys
+    lib, asan = hc_ubsan
     env = dict(os.environ, UBSAN_OPTIONS="print_stacktrace=1:halt_on_error=1",
                PYTHONPATH=os.pathsep.join([ROOT, os.environ.get("PYTHONPATH", "")]))
-    r = subprocess.run([sys.executable, os.path.abspath(__file__), hc_ubsan], cwd=ROOT, env=env,
+    if asan:
+        env.update(LD_PRELOAD=asan, ASAN_OPTIONS="detect_leaks=0")
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), lib], cwd=ROOT, env=env,
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, (r.stdout + r.stderr)[-4000:]
-
-
-if __name__ == "__main__":
-    import sys
-    _decode_all(sys.argv[1])
 
 
 def test_demuxer_on_damaged_streams_under_address_sanitizer(tmp_path):
@@ -139,3 +169,8 @@ def test_demuxer_on_damaged_streams_under_address_sanitizer(tmp_path):
         assert got == ["ok", str(ix["play48"]), str(ix["channels"]), str(len(ix["packets"])), str(len(chains)),
                        str(sum(c[3] for c in chains))], i
     assert accepted > 200
+
+
+if __name__ == "__main__":
+    import sys
+    _decode_all(sys.argv[1])
