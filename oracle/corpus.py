@@ -59,7 +59,7 @@ def ref_lib():
     global _lib
     if _lib is None:
         if not os.path.exists(REF_LIB):
-            raise OSError("oracle/_ref/libopus_ref.so is missing: run make -C oracle")
+            raise OSError("oracle/_ref/libopus_ref.so is missing: run make -C oracle REF=<reference tree>")
         lib = ctypes.CDLL(REF_LIB)
         lib.oref_encode.restype = ctypes.c_int
         lib.oref_encode.argtypes = [

@@ -2,7 +2,7 @@
 has the reference tree; the fixtures are committed and nothing reads the
 reference at test time).
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py <reference source tree>
 
 What it writes (all small):
   streams/*.opus    seeded synthetic Ogg Opus streams from the vendored libopus
@@ -100,7 +100,9 @@ def code3_stream():
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference source tree>")
+    ref_root = sys.argv[1]
     ogg_index = _load("ref_ogg_index", os.path.join(ref_root, "ogg_index.py"))
     gpu_resample = _load("ref_gpu_resample", os.path.join(ref_root, "gpu_resample.py"))
     import torch
