@@ -424,169 +424,506 @@ int run_blob(const char *blob_path, const char *chains_path, const char *out, un
 }
 
 // ------------------------------------------------------------------ daemon
+//
+// The daemon is an event loop over the listening socket and every open client
+// connection at once (poll), with the decoding handed to the library's
+// continuous-batching server (cuopus_server_*).  A connection's request line
+// is parsed into a Request; a DECODE request's file is read, probed and
+// submitted, and the connection is answered when the server completes it, so
+// requests from several clients are admitted together and decode in the same
+// waves on the GPU.  One server is kept per distinct (output format, chain
+// length, preroll, lanes per chain), created on first use and kept resident,
+// each with a device arena of CUOPUS_SERVE_BUDGET_MB (default 4096).
+//
+// Reply fields of OK, in order: int16 values (or float32 samples) written,
+// playable samples per channel at 48 kHz, decode ms (submit to completion in
+// the server: queueing, host->device copy, decode and resample), request wall
+// ms (line received to reply), file read + demux + submit ms, host->device
+// ms and resample ms (both 0.0: they are inside the decode ms), result copy
+// ms, file write ms.
+//
+// A connection that has not sent a complete line 30 s after it was accepted
+// is closed.  QUIT is answered at once; requests already submitted still
+// complete and are answered, then the daemon exits 0.  With no connection
+// open and nothing in flight for CUOPUS_SERVE_IDLE_S seconds (default 600) it
+// exits 0 as well.
 
-void reply(int fd, const std::string &msg)
+enum class Verb { None, Ping, Quit, Decode, Malformed, Unknown };
+
+struct Request {
+    Verb verb = Verb::None;
+    bool f16k = false;
+    double seg_s = 0, preroll_ms = 0;
+    unsigned stride = DEF_STRIDE;
+    std::string in, out;
+};
+
+// One request line -> Request.  Fields are separated by blanks; paths may not
+// contain blanks (the protocol's own limit).
+Request parse_request(const std::string &line)
+{
+    std::vector<std::string> tok;
+    size_t i = 0;
+    auto blank = [](char ch) { return ch == ' ' || ch == '\t' || ch == '\r'; };
+    while (i < line.size()) {
+        while (i < line.size() && blank(line[i])) i++;
+        size_t j = i;
+        while (j < line.size() && !blank(line[j])) j++;
+        if (j > i) tok.push_back(line.substr(i, j - i));
+        i = j;
+    }
+    Request r;
+    if (tok.empty()) return r;
+    r.verb = Verb::Unknown;
+    if (tok[0] == "PING") {
+        r.verb = Verb::Ping;
+    } else if (tok[0] == "QUIT") {
+        r.verb = Verb::Quit;
+    } else if (tok[0] == "DECODE" || tok[0] == "DECODE16F") {
+        r.f16k = tok[0] == "DECODE16F";
+        r.verb = Verb::Malformed;
+        if (tok.size() != 6) return r;
+        char *end = nullptr;
+        r.seg_s = strtod(tok[1].c_str(), &end);
+        if (*end || !(r.seg_s > 0)) return r;
+        r.preroll_ms = strtod(tok[2].c_str(), &end);
+        if (*end || r.preroll_ms < 0) return r;
+        long st = strtol(tok[3].c_str(), &end, 10);
+        if (*end || st < 0) return r;
+        r.stride = (unsigned)(st < 1 ? 1 : st);
+        r.in = tok[4];
+        r.out = tok[5];
+        r.verb = Verb::Decode;
+    }
+    return r;
+}
+
+int width_of(unsigned stride)
+{
+    int w = 1;
+    while (w * 2 <= (int)stride && w < 32) w *= 2;
+    return w;
+}
+
+// Resident decode servers, one per request configuration.
+class ServerPool {
+  public:
+    ServerPool() = default;
+    ServerPool(const ServerPool &) = delete;
+    ServerPool &operator=(const ServerPool &) = delete;
+    ~ServerPool()
+    {
+        for (auto &e : servers_) cuopus_server_destroy(e.srv);
+    }
+
+    cuopus_server *get(const Request &r, std::string &err)
+    {
+        const int w = width_of(r.stride);
+        for (auto &e : servers_)
+            if (e.f16k == r.f16k && e.seg == r.seg_s && e.pre == r.preroll_ms && e.width == w) return e.srv;
+        cuopus_server_config cfg;
+        memset(&cfg, 0, sizeof cfg);
+        long long mb = 4096;
+        if (const char *v = getenv("CUOPUS_SERVE_BUDGET_MB"))
+            if (atoll(v) > 0) mb = atoll(v);
+        cfg.budget_bytes = (int64_t)mb << 20;
+        cfg.width = w;
+        cfg.seg_s = r.seg_s;
+        cfg.preroll_ms = r.preroll_ms;
+        cfg.f16k = r.f16k ? 1 : 0;
+        cuopus_server *s = nullptr;
+        char eb[512];
+        if (cuopus_server_create(&cfg, &s, eb, sizeof eb)) {
+            err = eb;
+            return nullptr;
+        }
+        servers_.push_back({r.f16k, r.seg_s, r.preroll_ms, w, s});
+        return s;
+    }
+
+  private:
+    struct Entry {
+        bool f16k;
+        double seg, pre;
+        int width;
+        cuopus_server *srv;
+    };
+    std::vector<Entry> servers_;
+};
+
+struct Client {
+    int fd = -1;
+    std::string inbuf;
+    double accepted_ms = 0;
+    double line_ms = 0;         // request line complete
+    bool in_server = false;     // a DECODE is submitted and not yet answered
+    cuopus_server *srv = nullptr;
+    uint64_t id = 0;
+    Request req;
+    size_t out_bytes = 0;
+    std::vector<uint8_t> host;  // the result, copied out by the server
+    long long play48 = 0;
+    double prep_ms = 0;
+    bool done = false;          // answered: close and drop
+};
+
+bool send_all(int fd, const std::string &msg)
 {
     size_t o = 0;
     while (o < msg.size()) {
-        ssize_t w = write(fd, msg.data() + o, msg.size() - o);
-        if (w <= 0) break;
+        ssize_t w = send(fd, msg.data() + o, msg.size() - o, MSG_NOSIGNAL);
+        if (w < 0 && errno == EINTR) continue;
+        if (w <= 0) return false;
         o += (size_t)w;
+    }
+    return true;
+}
+
+class Daemon {
+  public:
+    Daemon(const char *path, int idle_s) : path_(path), idle_s_(idle_s) {}
+    int run();
+
+  private:
+    bool listen_on_path();
+    void on_readable(Client &c);
+    void on_line(Client &c, const std::string &line);
+    void submit(Client &c);
+    void collect();
+    void answer(Client &c, const std::string &text);
+
+    static const size_t kMaxLine = 8192;
+    static constexpr double kLineTimeoutMs = 30000.0;
+    std::string path_;
+    int idle_s_;
+    int lfd_ = -1;
+    bool quitting_ = false;
+    double last_busy_ms_ = 0;
+    std::vector<Client> clients_;
+    ServerPool pool_;
+};
+
+bool Daemon::listen_on_path()
+{
+    struct sockaddr_un addr;
+    memset(&addr, 0, sizeof addr);
+    if (path_.size() >= sizeof(addr.sun_path)) {
+        fprintf(stderr, "cuopus_decode: socket path longer than %zu bytes\n", sizeof(addr.sun_path) - 1);
+        return false;
+    }
+    addr.sun_family = AF_UNIX;
+    memcpy(addr.sun_path, path_.c_str(), path_.size() + 1);
+    lfd_ = socket(AF_UNIX, SOCK_STREAM | SOCK_NONBLOCK, 0);
+    if (lfd_ < 0) {
+        perror("cuopus_decode: socket");
+        return false;
+    }
+    unlink(path_.c_str());
+    if (bind(lfd_, (struct sockaddr *)&addr, sizeof addr) != 0 || listen(lfd_, 64) != 0) {
+        perror("cuopus_decode: bind / listen");
+        close(lfd_);
+        lfd_ = -1;
+        return false;
+    }
+    return true;
+}
+
+void Daemon::answer(Client &c, const std::string &text)
+{
+    send_all(c.fd, text);
+    c.done = true;
+}
+
+void Daemon::on_readable(Client &c)
+{
+    char buf[4096];
+    ssize_t r = recv(c.fd, buf, sizeof buf, MSG_DONTWAIT);
+    if (r < 0 && (errno == EAGAIN || errno == EWOULDBLOCK || errno == EINTR)) return;
+    if (r <= 0) {               // closed before a full line: answer what there is
+        on_line(c, c.inbuf);
+        return;
+    }
+    c.inbuf.append(buf, (size_t)r);
+    size_t nl = c.inbuf.find('\n');
+    if (nl != std::string::npos) {
+        on_line(c, c.inbuf.substr(0, nl));
+    } else if (c.inbuf.size() >= kMaxLine) {
+        answer(c, "ERR request line too long\n");
     }
 }
 
-int run_serve(const char *sock_path)
+void Daemon::on_line(Client &c, const std::string &line)
 {
-    signal(SIGPIPE, SIG_IGN);
-    int idle_s = 600;
-    const char *e = getenv("CUOPUS_SERVE_IDLE_S");
-    if (e && atoi(e) > 0) idle_s = atoi(e);
-    struct sockaddr_un addr;
-    if (strlen(sock_path) >= sizeof(addr.sun_path)) {
-        fprintf(stderr, "cuopus_decode: socket path longer than %zu bytes\n", sizeof(addr.sun_path) - 1);
-        return 2;
+    c.line_ms = now_ms();
+    c.req = parse_request(line);
+    switch (c.req.verb) {
+    case Verb::Ping:
+        answer(c, "PONG 2\n");
+        break;
+    case Verb::Quit:
+        answer(c, "BYE\n");
+        quitting_ = true;
+        break;
+    case Verb::Decode:
+        submit(c);
+        break;
+    case Verb::Malformed:
+        answer(c, "ERR bad request\n");
+        break;
+    default:
+        answer(c, "ERR unknown command\n");
+        break;
     }
-    unlink(sock_path);
-    int srv = socket(AF_UNIX, SOCK_STREAM, 0);
-    if (srv < 0) {
-        perror("socket");
-        return 2;
+}
+
+void Daemon::submit(Client &c)
+{
+    std::string err;
+    std::vector<uint8_t> ogg;
+    if (!read_file(c.req.in.c_str(), ogg, err)) return answer(c, "ERR " + err + "\n");
+    char eb[512];
+    int64_t play = 0, n16 = 0;
+    int32_t ch = 0;
+    if (cuopus_probe_pcm(ogg.data(), ogg.size(), &play, &ch, eb, sizeof eb)) return answer(c, std::string("ERR ") + eb + "\n");
+    if (c.req.f16k) {
+        if (ch != 1) return answer(c, "ERR only mono supported with DECODE16F\n");
+        if (cuopus_probe(ogg.data(), ogg.size(), &n16, eb, sizeof eb)) return answer(c, std::string("ERR ") + eb + "\n");
+        c.out_bytes = 4 * (size_t)n16;
+    } else {
+        c.out_bytes = 2 * (size_t)play * (size_t)ch;
     }
-    memset(&addr, 0, sizeof addr);
-    addr.sun_family = AF_UNIX;
-    strncpy(addr.sun_path, sock_path, sizeof(addr.sun_path) - 1);
-    if (bind(srv, (struct sockaddr *)&addr, sizeof addr) < 0) {
-        perror("bind");
-        return 2;
+    c.play48 = play;
+    c.srv = pool_.get(c.req, err);
+    if (!c.srv) return answer(c, "ERR " + err + "\n");
+    if (cuopus_server_submit(c.srv, ogg.data(), ogg.size(), &c.id, eb, sizeof eb))
+        return answer(c, std::string("ERR ") + eb + "\n");
+    c.host.resize(c.out_bytes ? c.out_bytes : 1);
+    c.in_server = true;
+    c.prep_ms = now_ms() - c.line_ms;
+}
+
+// Answer every submitted request the server has completed.
+void Daemon::collect()
+{
+    for (Client &c : clients_) {
+        if (!c.in_server) continue;
+        int64_t nout = 0;
+        int32_t ch = 0;
+        double lat = 0;
+        char eb[512];
+        double t0 = now_ms();
+        int rc = cuopus_server_wait(c.srv, c.id, 0, c.host.data(), c.host.size(), &nout, &ch, &lat, eb, sizeof eb);
+        if (rc == 4) continue;   // still decoding
+        double copy_ms = now_ms() - t0;
+        c.in_server = false;
+        if (rc) {
+            answer(c, std::string("ERR ") + eb + "\n");
+            continue;
+        }
+        std::string err;
+        double t1 = now_ms();
+        bool wrote = write_file(c.req.out.c_str(), c.host.data(), c.out_bytes, err);
+        std::vector<uint8_t>().swap(c.host);
+        if (!wrote) {
+            answer(c, "ERR " + err + "\n");
+            continue;
+        }
+        double write_ms = now_ms() - t1;
+        unsigned long long values = c.req.f16k ? (unsigned long long)nout : (unsigned long long)nout * (unsigned)ch;
+        char r[400];
+        snprintf(r, sizeof r, "OK %llu %lld %.1f %.1f %.1f %.1f %.1f %.1f %.1f\n", values, c.play48, lat,
+                 now_ms() - c.line_ms, c.prep_ms, 0.0, copy_ms, 0.0, write_ms);
+        answer(c, r);
     }
-    if (listen(srv, 16) < 0) {
-        perror("listen");
-        return 2;
-    }
+}
+
+int Daemon::run()
+{
+    if (!listen_on_path()) return 2;
     double t0 = now_ms();
     char eb[512];
     if (cuopus_warmup(eb, sizeof eb)) fprintf(stderr, "cuopus_decode: warmup: %s\n", eb);
-    fprintf(stderr, "cuopus_decode: serving on %s (warmup %.0f ms, idle exit %ds)\n", sock_path, now_ms() - t0,
-            idle_s);
-    std::vector<char> line(8192);
+    fprintf(stderr, "cuopus_decode: serving on %s (warmup %.0f ms, idle exit %ds)\n", path_.c_str(), now_ms() - t0,
+            idle_s_);
+    last_busy_ms_ = now_ms();
     for (;;) {
-        struct pollfd pfd = {srv, POLLIN, 0};
-        int pr = poll(&pfd, 1, idle_s * 1000);
-        if (pr == 0) {
-            fprintf(stderr, "cuopus_decode: idle %ds, exiting\n", idle_s);
-            unlink(sock_path);
-            return 0;
+        bool busy = false;
+        for (const Client &c : clients_) busy = busy || c.in_server;
+        if (quitting_ && !busy) break;
+        if (!clients_.empty()) last_busy_ms_ = now_ms();
+        else if (now_ms() - last_busy_ms_ > idle_s_ * 1000.0) {
+            fprintf(stderr, "cuopus_decode: idle %ds, exiting\n", idle_s_);
+            break;
         }
-        if (pr < 0) {
-            if (errno == EINTR) continue;
-            perror("poll");
-            return 2;
+        std::vector<struct pollfd> pf;
+        if (!quitting_) pf.push_back({lfd_, POLLIN, 0});
+        std::vector<size_t> who;
+        for (size_t i = 0; i < clients_.size(); i++)
+            if (!clients_[i].in_server && !clients_[i].done) {
+                pf.push_back({clients_[i].fd, POLLIN, 0});
+                who.push_back(i);
+            }
+        // decodes in flight: come back soon to collect them; otherwise wake at
+        // least once a second for the line and idle timeouts
+        int wait_ms = busy ? 2 : 1000;
+        int pr = poll(pf.data(), pf.size(), wait_ms);
+        if (pr < 0 && errno != EINTR) {
+            perror("cuopus_decode: poll");
+            break;
         }
-        int fd = accept(srv, nullptr, nullptr);
-        if (fd < 0) continue;
-        // A client that connects and sends no request line must not hold the
-        // single-threaded loop: its read gives up after 30 s.
-        struct timeval rto = {30, 0};
-        setsockopt(fd, SOL_SOCKET, SO_RCVTIMEO, &rto, sizeof rto);
-        size_t got = 0;
-        while (got < line.size() - 1) {
-            ssize_t r = read(fd, line.data() + got, line.size() - 1 - got);
-            if (r <= 0) break;
-            got += (size_t)r;
-            if (memchr(line.data(), '\n', got)) break;
-        }
-        line[got] = 0;
-        char *nl = strchr(line.data(), '\n');
-        if (nl) *nl = 0;
-        const char *ln = line.data();
-        int mode16 = -1;
-        const char *args = nullptr;
-        if (!strncmp(ln, "DECODE16F ", 10)) {
-            mode16 = 1;
-            args = ln + 10;
-        } else if (!strncmp(ln, "DECODE ", 7)) {
-            mode16 = 0;
-            args = ln + 7;
-        }
-        if (!strncmp(ln, "PING", 4)) {
-            reply(fd, "PONG 2\n");
-        } else if (!strncmp(ln, "QUIT", 4)) {
-            reply(fd, "BYE\n");
-            close(fd);
-            unlink(sock_path);
-            return 0;
-        } else if (mode16 >= 0) {
-            double seg_s = 0, preroll_ms = 0;
-            unsigned stride = DEF_STRIDE;
-            std::vector<char> ogg(4096), out(4096);
-            if (sscanf(args, "%lf %lf %u %4095s %4095s", &seg_s, &preroll_ms, &stride, ogg.data(), out.data()) != 5) {
-                reply(fd, "ERR bad request\n");
-            } else {
-                double rt0 = now_ms();
-                std::string err;
-                std::vector<uint8_t> data;
-                Report rep;
-                int rc = read_file(ogg.data(), data, err) ? 0 : 2;
-                double read_ms = now_ms() - rt0;
-                if (!rc) {
-                    set_env_params(seg_s, preroll_ms, stride);
-                    rc = decode_ogg(data, out.data(), mode16 == 1, rep, err);
-                }
-                if (!rc) {
-                    char r[400];
-                    snprintf(r, sizeof r, "OK %llu %lld %.1f %.1f %.1f %.1f %.1f %.1f %.1f\n", rep.out_samples,
-                             rep.play48, rep.st.kernel_ms, now_ms() - rt0, read_ms + rep.st.demux_ms,
-                             rep.st.h2d_ms, rep.d2h_ms, rep.st.resample_ms, rep.fwrite_ms);
-                    reply(fd, r);
-                } else {
-                    reply(fd, "ERR " + err + "\n");
+        size_t base = quitting_ ? 0 : 1;
+        if (pr > 0) {
+            for (size_t k = 0; k < who.size(); k++)
+                if (pf[base + k].revents & (POLLIN | POLLHUP | POLLERR)) on_readable(clients_[who[k]]);
+            if (!quitting_ && (pf[0].revents & POLLIN)) {
+                for (;;) {
+                    int fd = accept(lfd_, nullptr, nullptr);
+                    if (fd < 0) break;
+                    Client c;
+                    c.fd = fd;
+                    c.accepted_ms = now_ms();
+                    clients_.push_back(std::move(c));
                 }
             }
-        } else {
-            reply(fd, "ERR unknown command\n");
         }
-        close(fd);
+        collect();
+        double now = now_ms();
+        for (Client &c : clients_)
+            if (!c.done && !c.in_server && now - c.accepted_ms > kLineTimeoutMs) answer(c, "ERR no request line\n");
+        for (size_t i = 0; i < clients_.size();) {
+            if (clients_[i].done) {
+                close(clients_[i].fd);
+                clients_.erase(clients_.begin() + (long)i);
+            } else {
+                i++;
+            }
+        }
     }
+    for (Client &c : clients_) close(c.fd);
+    clients_.clear();
+    close(lfd_);
+    unlink(path_.c_str());
+    return 0;
+}
+
+// ------------------------------------------------------------------ command line
+//
+// Three modes: --serve <socket>, --ogg <in> [out|-] [options], and the legacy
+// blob mode <packets.blob> <chains.bin> <out.pcm> [stride].  Options are read
+// from one table; an argument that does not start with "--", or is "-",
+// is positional.
+
+struct CliArgs {
+    std::vector<const char *> pos;
+    double seg_s = 1.0, preroll_ms = DEF_PREROLL_MS;
+    long stride = DEF_STRIDE;
+    bool f16k = false, serve = false, ogg = false;
+    const char *dump_blob = nullptr, *dump_chains = nullptr;
+};
+
+bool num(const char *v, double &out)
+{
+    char *end = nullptr;
+    out = strtod(v, &end);
+    return end != v && !*end;
+}
+
+// One entry per option: its name, whether it takes a value, and how it sets
+// the arguments (false: the value does not parse).
+struct OptSpec {
+    const char *name;
+    bool takes_value;
+    bool (*apply)(CliArgs &, const char *);
+};
+
+const OptSpec kOpts[] = {
+    {"--serve", false, [](CliArgs &a, const char *) { return a.serve = true; }},
+    {"--ogg", false, [](CliArgs &a, const char *) { return a.ogg = true; }},
+    {"--f16k", false, [](CliArgs &a, const char *) { return a.f16k = true; }},
+    {"--seg", true, [](CliArgs &a, const char *v) { return num(v, a.seg_s); }},
+    {"--preroll", true, [](CliArgs &a, const char *v) { return num(v, a.preroll_ms); }},
+    {"--stride", true,
+     [](CliArgs &a, const char *v) {
+         double d = 0;
+         bool ok = num(v, d);
+         a.stride = (long)d;
+         return ok;
+     }},
+    {"--dump-blob", true, [](CliArgs &a, const char *v) { return (a.dump_blob = v) != nullptr; }},
+    {"--dump-chains", true, [](CliArgs &a, const char *v) { return (a.dump_chains = v) != nullptr; }},
+};
+
+bool parse_args(int argc, char **argv, CliArgs &a, std::string &err)
+{
+    for (int i = 1; i < argc; i++) {
+        const char *s = argv[i];
+        if (strncmp(s, "--", 2) != 0) {
+            a.pos.push_back(s);
+            continue;
+        }
+        const OptSpec *o = nullptr;
+        for (const OptSpec &c : kOpts)
+            if (!strcmp(c.name, s)) o = &c;
+        if (!o) {
+            err = std::string("unknown option ") + s;
+            return false;
+        }
+        const char *v = nullptr;
+        if (o->takes_value) {
+            if (i + 1 >= argc) {
+                err = std::string(s) + " needs a value";
+                return false;
+            }
+            v = argv[++i];
+        }
+        if (!o->apply(a, v)) {
+            err = std::string("bad value for ") + s + ": " + (v ? v : "");
+            return false;
+        }
+    }
+    if (a.stride < 1) a.stride = 1;
+    return true;
+}
+
+int usage(const char *prog)
+{
+    fprintf(stderr,
+            "usage: %s <packets.blob> <chains.bin> <out.pcm> [stride]\n"
+            "       %s --ogg <in.ogg> [out.pcm|-] [--seg S] [--preroll MS] [--stride N] [--f16k]\n"
+            "                 [--dump-blob F] [--dump-chains F]\n"
+            "       %s --serve <unix_socket>\n",
+            prog, prog, prog);
+    return 2;
 }
 
 } // namespace
 
 int main(int argc, char **argv)
 {
-    if (argc >= 3 && !strcmp(argv[1], "--serve")) return run_serve(argv[2]);
-    if (argc >= 3 && !strcmp(argv[1], "--ogg")) {
-        const char *ogg = argv[2];
-        const char *out = nullptr, *dump_blob = nullptr, *dump_chains = nullptr;
-        double seg_s = 1.0, preroll_ms = DEF_PREROLL_MS;
-        unsigned stride = DEF_STRIDE;
-        bool f16k = false;
-        int ai = 3;
-        if (ai < argc && (argv[ai][0] != '-' || !strcmp(argv[ai], "-"))) out = argv[ai++];
-        for (; ai < argc; ai++) {
-            if (!strcmp(argv[ai], "--seg") && ai + 1 < argc) seg_s = atof(argv[++ai]);
-            else if (!strcmp(argv[ai], "--preroll") && ai + 1 < argc) preroll_ms = atof(argv[++ai]);
-            else if (!strcmp(argv[ai], "--stride") && ai + 1 < argc) stride = (unsigned)atoi(argv[++ai]);
-            else if (!strcmp(argv[ai], "--f16k")) f16k = true;
-            else if (!strcmp(argv[ai], "--dump-blob") && ai + 1 < argc) dump_blob = argv[++ai];
-            else if (!strcmp(argv[ai], "--dump-chains") && ai + 1 < argc) dump_chains = argv[++ai];
-            else {
-                fprintf(stderr, "cuopus_decode: unknown option %s\n", argv[ai]);
-                return 2;
-            }
-        }
-        if (stride < 1) stride = 1;
-        return run_ogg_once(ogg, out, seg_s, preroll_ms, stride, f16k, dump_blob, dump_chains);
-    }
-    if (argc < 4) {
-        fprintf(stderr,
-                "usage: %s <packets.blob> <chains.bin> <out.pcm> [stride]\n"
-                "       %s --ogg <in.ogg> [out.pcm|-] [--seg S] [--preroll MS] [--stride N] [--f16k]\n"
-                "                 [--dump-blob F] [--dump-chains F]\n"
-                "       %s --serve <unix_socket>\n",
-                argv[0], argv[0], argv[0]);
+    CliArgs a;
+    std::string err;
+    if (!parse_args(argc, argv, a, err)) {
+        fprintf(stderr, "cuopus_decode: %s\n", err.c_str());
         return 2;
     }
-    unsigned stride = argc > 4 ? (unsigned)atoi(argv[4]) : DEF_STRIDE;
-    if (stride < 1) stride = 1;
-    return run_blob(argv[1], argv[2], argv[3], stride);
+    if (a.serve) {
+        if (a.pos.size() != 1) return usage(argv[0]);
+        int idle_s = 600;
+        if (const char *e = getenv("CUOPUS_SERVE_IDLE_S"))
+            if (atoi(e) > 0) idle_s = atoi(e);
+        Daemon d(a.pos[0], idle_s);
+        return d.run();
+    }
+    if (a.ogg) {
+        if (a.pos.empty() || a.pos.size() > 2) return usage(argv[0]);
+        return run_ogg_once(a.pos[0], a.pos.size() > 1 ? a.pos[1] : nullptr, a.seg_s, a.preroll_ms,
+                            (unsigned)a.stride, a.f16k, a.dump_blob, a.dump_chains);
+    }
+    if (a.pos.size() < 3 || a.pos.size() > 4) return usage(argv[0]);
+    unsigned stride = DEF_STRIDE;
+    if (a.pos.size() == 4) {
+        long v = strtol(a.pos[3], nullptr, 10);
+        stride = (unsigned)(v < 1 ? 1 : v);
+    }
+    return run_blob(a.pos[0], a.pos[1], a.pos[2], stride);
 }

@@ -54,6 +54,19 @@ def test_demux_dumps_match_reference_tables(cli, name, tmp_path):
     assert tab == g["chains_0.5_80"]
 
 
+def test_arguments(cli, tmp_path):
+    """Options may come before or after the output path; bad values and
+    unknown options are usage errors (exit 2)."""
+    r = subprocess.run([cli, "--ogg", _path("plain_a"), "--seg", "0.5", "-"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert "chains" in r.stdout
+    for bad in (["--stride", "x"], ["--seg"], ["--bogus"]):
+        r = subprocess.run([cli, "--ogg", _path("plain_a"), "-"] + bad, capture_output=True, text=True)
+        assert r.returncode == 2, bad
+    r = subprocess.run([cli, "--serve"], capture_output=True, text=True)
+    assert r.returncode == 2 and "usage" in r.stderr
+
+
 def test_bad_file(cli, tmp_path):
     p = tmp_path / "x.opus"
     p.write_bytes(b"not an ogg file")
@@ -77,9 +90,28 @@ def test_daemon_protocol_without_decoding(cli):
             time.sleep(0.1)
         time.sleep(0.2)
         assert _ask(sock, "PING") == "PONG 2"
+        # a client that connects and sends nothing does not hold up the others,
+        # and a line sent in pieces is read whole
+        idle = socket.socket(socket.AF_UNIX, socket.SOCK_STREAM)
+        idle.connect(sock)
+        part = socket.socket(socket.AF_UNIX, socket.SOCK_STREAM)
+        part.settimeout(60)
+        part.connect(sock)
+        part.sendall(b"PI")
+        assert _ask(sock, "PING") == "PONG 2"
+        time.sleep(0.1)
+        part.sendall(b"NG\n")
+        assert part.recv(64) == b"PONG 2\n"
+        part.close()
         assert _ask(sock, "DECODE 1 250 32 /nonexistent %s" % os.path.join(d, "o")).startswith("ERR")
+        bad = os.path.join(d, "bad.opus")
+        with open(bad, "wb") as f:
+            f.write(b"not an ogg stream")
+        assert _ask(sock, "DECODE 1 250 32 %s %s" % (bad, os.path.join(d, "o"))).startswith("ERR")
         assert _ask(sock, "DECODE16F 1 250").startswith("ERR bad request")
+        assert _ask(sock, "DECODE 1 x 32 a b").startswith("ERR bad request")
         assert _ask(sock, "BOGUS").startswith("ERR")
+        idle.close()
         assert _ask(sock, "QUIT") == "BYE"
         assert p.wait(timeout=30) == 0
         assert not os.path.exists(sock)
