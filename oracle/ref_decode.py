@@ -72,3 +72,34 @@ def decode_chains(packets, chains, channels, nthreads=None, want_pcm=True, fec=0
 def _toc(p):
     from .ogg_port import decode_capacity48
     return decode_capacity48(p)
+
+
+def check_batch(data, off, lens, first, npkts, chans, trim, keep, got_pcm, got_off, got_res, nthreads=None):
+    """Full-size parity of a decoded batch against libopus (oref_check_chains):
+    every chain decoded afresh and compared in place with the batch under test
+    (int16 PCM of its keep window at got_off, and the {stop, samples,
+    final_range} of its result record got_res [n, 4] uint32).  All arrays are
+    host numpy arrays laid out as the decoder's chain table.  Returns dict
+    with per-chain differing sample counts (bad) and flags (bit 0 stop, bit 1
+    samples, bit 2 final range)."""
+    lib = ref_lib()
+    fn = lib.oref_check_chains
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p] * 6 + [ctypes.c_int] + [ctypes.c_void_p] * 7 + [ctypes.c_int]
+    c = lambda a, dt: np.ascontiguousarray(a, dtype=dt)
+    data, off, lens = c(data, np.uint8), c(off, np.uint64), c(lens, np.uint32)
+    first, npkts, chans = c(first, np.uint32), c(npkts, np.uint32), c(chans, np.uint8)
+    trim, keep, got_off = c(trim, np.uint64), c(keep, np.uint64), c(got_off, np.uint64)
+    got_pcm, got_res = c(got_pcm, np.int16), c(got_res, np.uint32)
+    n = len(first)
+    assert got_res.size >= 4 * n
+    need = int((keep * chans.astype(np.uint64) + got_off).max()) if n else 0
+    assert got_pcm.size >= need, "PCM buffer shorter than the chain table's windows"
+    bad = np.zeros(max(n, 1), np.uint64)
+    flags = np.zeros(max(n, 1), np.uint32)
+    rc = fn(data.ctypes.data, off.ctypes.data, lens.ctypes.data, first.ctypes.data, npkts.ctypes.data,
+            chans.ctypes.data, n, trim.ctypes.data, keep.ctypes.data, got_pcm.ctypes.data, got_off.ctypes.data,
+            got_res.ctypes.data, bad.ctypes.data, flags.ctypes.data, nthreads or (os.cpu_count() or 1))
+    if rc != 0:
+        raise RuntimeError("oref_check_chains failed to start threads")
+    return dict(bad=bad[:n], flags=flags[:n])

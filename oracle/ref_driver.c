@@ -148,6 +148,105 @@ int oref_decode_chains_fec(const uint8_t *data, const uint64_t *off, const uint3
     return rc;
 }
 
+/* ------------------------------------------------------------------ full-size check
+ *
+ * oref_check_chains: the parity check of a whole decoded batch, for batches
+ * whose PCM is too large to hold twice.  Every chain is decoded with a fresh
+ * OpusDecoder(48000, chans[c]) under the chain protocol above (decode_fec = 0)
+ * and compared, packet by packet, against the batch under test: the samples
+ * of its keep window [trim, trim + keep) against got_pcm + got_off[c]
+ * (interleaved int16), and at the end the stop status, the samples decoded
+ * and the final range against got_res[4c + 0..2] ({stop, samples,
+ * final_range, time}, the decoder's per-chain result record).  bad[c]
+ * receives the number of differing int16 values of chain c; flags[c] bit 0 a
+ * different stop status, bit 1 a different sample count, bit 2 a different
+ * final range.  Chains run on a pthread pool.  Returns 0, or -1 when no thread
+ * could start. */
+typedef struct {
+    const uint8_t *data;
+    const uint64_t *off;
+    const uint32_t *len;
+    const uint32_t *first, *npkts;
+    const uint8_t *chans;
+    const uint64_t *trim, *keep, *got_off;
+    const int16_t *got_pcm;
+    const uint32_t *got_res;
+    uint64_t *bad;
+    uint32_t *flags;
+    int nchains;
+    volatile int next;
+    pthread_mutex_t mu;
+} oref_check_job;
+
+static void *oref_check_worker(void *arg)
+{
+    oref_check_job *j = (oref_check_job *)arg;
+    OpusDecoder *dec = (OpusDecoder *)malloc((size_t)opus_decoder_get_size(2));
+    int16_t *buf = (int16_t *)malloc(sizeof(int16_t) * OREF_MAX_PKT_SAMPLES * 2);
+    if (!dec || !buf) { free(dec); free(buf); return NULL; }
+    for (;;) {
+        pthread_mutex_lock(&j->mu);
+        int c = j->next++;
+        pthread_mutex_unlock(&j->mu);
+        if (c >= j->nchains) break;
+        int ch = j->chans[c];
+        int32_t status = opus_decoder_init(dec, 48000, ch);
+        uint64_t pos = 0, bad = 0;
+        opus_uint32 rng = 0;
+        const uint64_t lo = j->trim[c], hi = j->trim[c] + j->keep[c];
+        const int16_t *got = j->got_pcm + j->got_off[c];
+        if (status == 0) {
+            for (uint32_t k = 0; k < j->npkts[c]; k++) {
+                uint64_t p = (uint64_t)j->first[c] + k;
+                int ret = opus_decode(dec, j->data + j->off[p], (opus_int32)j->len[p], buf, OREF_MAX_PKT_SAMPLES, 0);
+                if (ret < 0) { status = ret; break; }
+                opus_decoder_ctl(dec, OPUS_GET_FINAL_RANGE(&rng));
+                uint64_t a = pos > lo ? pos : lo, b = pos + (uint64_t)ret < hi ? pos + (uint64_t)ret : hi;
+                for (uint64_t t = a; t < b; t++)
+                    for (int q = 0; q < ch; q++)
+                        bad += buf[(t - pos) * (uint64_t)ch + (uint64_t)q] != got[(t - lo) * (uint64_t)ch + (uint64_t)q];
+                pos += (uint64_t)ret;
+            }
+        }
+        if (pos < hi) bad += (hi - (pos > lo ? pos : lo)) * (uint64_t)ch;   /* window not covered */
+        const uint32_t *r = j->got_res + 4 * (uint64_t)c;
+        uint32_t f = 0;
+        if ((int32_t)r[0] != status) f |= 1u;
+        if ((uint64_t)r[1] != pos) f |= 2u;
+        if (r[2] != (uint32_t)rng) f |= 4u;
+        j->bad[c] = bad;
+        j->flags[c] = f;
+    }
+    free(dec);
+    free(buf);
+    return NULL;
+}
+
+int oref_check_chains(const uint8_t *data, const uint64_t *off, const uint32_t *len, const uint32_t *first,
+                      const uint32_t *npkts, const uint8_t *chans, int nchains, const uint64_t *trim,
+                      const uint64_t *keep, const int16_t *got_pcm, const uint64_t *got_off,
+                      const uint32_t *got_res, uint64_t *bad, uint32_t *flags, int nthreads)
+{
+    oref_check_job j;
+    memset(&j, 0, sizeof(j));
+    j.data = data; j.off = off; j.len = len; j.first = first; j.npkts = npkts; j.chans = chans;
+    j.trim = trim; j.keep = keep; j.got_off = got_off; j.got_pcm = got_pcm; j.got_res = got_res;
+    j.bad = bad; j.flags = flags; j.nchains = nchains; j.next = 0;
+    pthread_mutex_init(&j.mu, NULL);
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 1024) nthreads = 1024;
+    pthread_t th[1024];
+    int started = 0, rc = 0;
+    for (int t = 0; t < nthreads; t++) {
+        if (pthread_create(&th[t], NULL, oref_check_worker, &j) != 0) { rc = -1; break; }
+        started++;
+    }
+    if (started == 0) oref_check_worker(&j);
+    for (int t = 0; t < started; t++) pthread_join(th[t], NULL);
+    pthread_mutex_destroy(&j.mu);
+    return started == 0 && nchains > 0 && rc ? -1 : 0;
+}
+
 /* ------------------------------------------------------------------ encode */
 
 typedef struct {

@@ -139,3 +139,50 @@ def test_libopus_range_decoder_gate():
         lib.oref_ec_schedule2(ctypes.c_void_p(arr.ctypes.data), len(b), ctypes.c_void_p(o2.ctypes.data))
         assert [int(x) for x in o1] == case["gate"]
         assert [int(x) for x in o2] == case["wide"]
+
+
+def test_full_size_check_finds_planted_differences():
+    """oref_check_chains, the full-size parity check the benchmark runs after
+    its timed region: on a batch laid out as the decoder's chain table it must
+    report nothing for libopus's own output, and exactly the differences
+    planted into a copy of it (one sample, one final range, one sample count,
+    one stop status)."""
+    from oracle import ref_decode
+    names = ["mixed_stereo_a", "mixed_mono_b", "long_hybrid", "code3_120ms"]
+    data, off, lens, first, npk, chans, trim, keep, res, pcm, got_off = [], [], [], [], [], [], [], [], [], [], []
+    base_p = base_b = base_o = 0
+    for nm in names:
+        ix = ogg_port.demux(_stream(nm))
+        pk, ch = ix["packets"], ix["channels"]
+        chains = ogg_port.build_chains(ix, 0.5, 250.0)
+        ref = ref_decode.decode_chains(pk, chains, ch)
+        for p in pk:
+            off.append(base_b)
+            lens.append(len(p))
+            base_b += len(p)
+        data.append(b"".join(pk))
+        for i, (f, n, t, k) in enumerate(chains):
+            first.append(f + base_p)
+            npk.append(n)
+            chans.append(ch)
+            trim.append(t)
+            keep.append(k)
+            res.append([0, int(ref["samples"][i]), int(ref["rng"][i][-1]), 1])
+            pcm.append(ref["pcm"][i][t * ch:(t + k) * ch])
+            got_off.append(base_o)
+            base_o += k * ch
+        base_p += len(pk)
+    blob = np.frombuffer(b"".join(data) + b"\0" * 16, np.uint8)
+    got = np.concatenate(pcm)
+    res = np.array(res, np.uint32)
+    args = (blob, off, lens, first, npk, chans, trim, keep)
+    r = ref_decode.check_batch(*args, got, got_off, res)
+    assert len(first) > 20 and not r["bad"].any() and not r["flags"].any()
+    got2, res2 = got.copy(), res.copy()
+    got2[got_off[5] + 3] ^= 1
+    res2[7, 2] ^= 0x100
+    res2[9, 1] += 1
+    res2[11, 0] = np.uint32(0xFFFFFFFC)   # -4, OPUS_INVALID_PACKET
+    r = ref_decode.check_batch(*args, got2, got_off, res2)
+    assert np.flatnonzero(r["bad"]).tolist() == [5] and int(r["bad"][5]) == 1
+    assert {int(i): int(r["flags"][i]) for i in np.flatnonzero(r["flags"])} == {7: 4, 9: 2, 11: 1}
