@@ -3,9 +3,12 @@
   cuopus_b200/lib/libcuopus.so            the product: CUDA kernels for sm_100a
                                           plus the C ABI of include/cuopus.h
   cuopus_b200/lib/libcuopus_phases.so     the same with the decoder's stage timers
-                                          (diagnostics: python -m cuopus_b200.phase_profile)
+                                          (diagnostics: python bench.py --phases)
   cuopus_b200/lib/libcuopus_hostcheck.so  the same decoder sources compiled for
                                           the host (g++), used only by tests
+  cuopus_b200/lib/libcuopus_lanesim.so    the host build with every lane of a
+                                          group as a fiber, switched at random
+                                          points (tests of the lane discipline)
   cuopus_b200/bin/cuopus_decode           the command-line tool / daemon
 
 python -m cuopus_b200.build [--force]
@@ -29,6 +32,7 @@ LIBCUOPUS = os.path.join(LIB, "libcuopus.so")
 LIBPHASES = os.path.join(LIB, "libcuopus_phases.so")
 HOSTCHECK = os.path.join(LIB, "libcuopus_hostcheck.so")
 HOSTCHECK_REV = os.path.join(LIB, "libcuopus_hostcheck_rev.so")
+LANESIM = os.path.join(LIB, "libcuopus_lanesim.so")
 CLI = os.path.join(BIN, "cuopus_decode")
 
 
@@ -99,6 +103,17 @@ def build_hostcheck(force=False):
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-w", "-I", CSRC, *extra,
               os.path.join(CSRC, "hostcheck.cpp"), "-o", tmp, "-lpthread"])
         os.replace(tmp, target)
+    # the lane-interleaving build (lanesim.cpp): each lane a fiber, switched
+    # at function entries (-finstrument-functions; -Bsymbolic binds the entry
+    # hook to the library's own, not libc's empty one)
+    deps = _sources("lanesim.cpp", "dec")
+    if force or _stale(LANESIM, deps):
+        os.makedirs(LIB, exist_ok=True)
+        tmp = LANESIM + ".tmp"
+        _run(["g++", "-O1", "-g", "-fno-omit-frame-pointer", "-std=c++17", "-fPIC", "-shared", "-w", "-I", CSRC,
+              "-DCUO_LANE_SIM", "-finstrument-functions", os.path.join(CSRC, "lanesim.cpp"), "-o", tmp,
+              "-lpthread", "-ldl", "-Wl,-Bsymbolic"])
+        os.replace(tmp, LANESIM)
     return HOSTCHECK
 
 

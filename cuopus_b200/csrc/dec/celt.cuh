@@ -2144,11 +2144,12 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
     int effEnd = end;
     if (effEnd > T_CELT_EFFEBANDS) effEnd = T_CELT_EFFEBANDS;
     if (data == 0 || len <= 1) {
-        celt_decode_lost(L, st, N, LM, w);
+        // concealment (mode transitions, lost packets): serial extrapolation
+        // and state updates in place, on the first lane as a group of one
+        lead(L, [&]() CUO_INLINE { celt_decode_lost(lone(L), st, N, LM, w); });
         deemphasis(L, out_syn[0], out_syn[1], pcm, N, CC, st->preemph_memD, accum);
         return frame_size;
     }
-    if (st->loss_duration == 0) st->skip_plc = 0;
     RangeDec _dec;
     if (dec == 0) {
         rd_init(&_dec, data, len);
@@ -2158,126 +2159,166 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
             *backgroundLogE = st->backgroundLogE;
     if (C == 1) {
         LFOR(L, i, 0, CELT_NB) oldBandE[i] = oldBandE[i] > oldBandE[CELT_NB + i] ? oldBandE[i] : oldBandE[CELT_NB + i];
-        lsync(L);
     }
-    int32_t total_bits = len * 8;
-    int32_t tell = rd_tell(dec);
-    int silence;
-    if (tell >= total_bits) silence = 1;
-    else if (tell == 1) silence = rd_bit_logp(dec, 15);
-    else silence = 0;
-    if (silence) {
-        tell = len * 8;
-        dec->nbits_total += tell - rd_tell(dec);
-    }
-    int16_t postfilter_gain = 0;
-    int postfilter_pitch = 0, postfilter_tapset = 0;
-    if (start == 0 && tell + 16 <= total_bits) {
-        if (rd_bit_logp(dec, 1)) {
-            int octave = (int)rd_uint(dec, 6);
-            postfilter_pitch = (16 << octave) + (int)rd_bits(dec, 4 + octave) - 1;
-            int qg = (int)rd_bits(dec, 3);
-            if (rd_tell(dec) + 2 <= total_bits) postfilter_tapset = rd_icdf(dec, T_celt_tapset_icdf, 2);
-            postfilter_gain = (int16_t)(3072 * (qg + 1));   // QCONST16(.09375f, 15)
-        }
-        tell = rd_tell(dec);
-    }
-    int isTransient;
-    if (LM > 0 && tell + 3 <= total_bits) {
-        isTransient = rd_bit_logp(dec, 3);
-        tell = rd_tell(dec);
-    } else {
-        isTransient = 0;
-    }
-    int shortBlocks = isTransient ? M : 0;
-    int intra_ener = tell + 3 <= total_bits ? rd_bit_logp(dec, 3) : 0;
-    if (!intra_ener && st->loss_duration != 0) energy_after_loss(st, start, end, LM);
-    PHASE_BEGIN(t_ce);
-    unquant_coarse_energy(start, end, oldBandE, intra_ener, dec, C, LM);
-    PHASE_END(PH_CELT_COARSE, t_ce, L.id);
     int32_t *tf_res = w->tf_res;
-    tf_decode(start, end, isTransient, tf_res, LM, dec);
-    tell = rd_tell(dec);
-    int spread_decision = SPREAD_NORMAL;
-    if (tell + 4 <= total_bits) spread_decision = rd_icdf(dec, T_celt_spread_icdf, 5);
-    int32_t *cap = w->cap, *offsets = w->offsets;
-    init_caps(cap, LM, C);
-    int dynalloc_logp = 6;
-    total_bits <<= 3;
-    tell = (int32_t)rd_tell_frac(dec);
-    for (int i = start; i < end; i++) {
-        int width = C * (eB[i + 1] - eB[i]) << LM;
-        int quanta = imin(width << 3, imax(6 << 3, width));
-        int dll = dynalloc_logp, boost = 0;
-        while (tell + (dll << 3) < total_bits && boost < cap[i]) {
-            int flag = rd_bit_logp(dec, dll);
-            tell = (int32_t)rd_tell_frac(dec);
-            if (!flag) break;
-            boost += quanta;
-            total_bits -= quanta;
-            dll = 1;
-        }
-        offsets[i] = boost;
-        if (boost > 0) dynalloc_logp = imax(2, dynalloc_logp - 1);
-    }
-    int alloc_trim = tell + (6 << 3) <= total_bits ? rd_icdf(dec, T_celt_trim_icdf, 7) : 5;
-    int32_t bits = (((int32_t)len * 8) << 3) - (int32_t)rd_tell_frac(dec) - 1;
-    int anti_collapse_rsv = isTransient && LM >= 2 && bits >= ((LM + 2) << 3) ? (1 << 3) : 0;
-    bits -= anti_collapse_rsv;
-    int intensity = 0, dual_stereo = 0;
-    int32_t balance;
     int32_t *pulses = w->pulses, *fine_quant = w->fine_quant, *fine_priority = w->fine_priority;
-    PHASE_BEGIN(t_al);
-    int codedBands = clt_compute_allocation(start, end, offsets, cap, alloc_trim, &intensity, &dual_stereo, bits,
-                                            &balance, pulses, fine_quant, fine_priority, C, LM, dec, w);
-    PHASE_END(PH_CELT_ALLOC, t_al, L.id);
-    unquant_fine_energy(start, end, oldBandE, fine_quant, dec, C);
+    // The frame header, the energies and the bit allocation: entropy decoding
+    // and state updates in place, on the first lane; every lane gets the
+    // outcome (the per-band tables stay in the scratch).
+    enum { H_SILENCE, H_PF_GAIN, H_PF_PITCH, H_PF_TAPSET, H_TRANSIENT, H_SPREAD, H_AC_RSV, H_INTENSITY, H_DUAL,
+           H_BALANCE, H_CODED, H_N };
+    int32_t hv[H_N] = {0};
+    lead_rd(L, dec, [&]() CUO_INLINE {
+        if (st->loss_duration == 0) st->skip_plc = 0;
+        int32_t total_bits = len * 8;
+        int32_t tell = rd_tell(dec);
+        int silence;
+        if (tell >= total_bits) silence = 1;
+        else if (tell == 1) silence = rd_bit_logp(dec, 15);
+        else silence = 0;
+        if (silence) {
+            tell = len * 8;
+            dec->nbits_total += tell - rd_tell(dec);
+        }
+        int16_t postfilter_gain = 0;
+        int postfilter_pitch = 0, postfilter_tapset = 0;
+        if (start == 0 && tell + 16 <= total_bits) {
+            if (rd_bit_logp(dec, 1)) {
+                int octave = (int)rd_uint(dec, 6);
+                postfilter_pitch = (16 << octave) + (int)rd_bits(dec, 4 + octave) - 1;
+                int qg = (int)rd_bits(dec, 3);
+                if (rd_tell(dec) + 2 <= total_bits) postfilter_tapset = rd_icdf(dec, T_celt_tapset_icdf, 2);
+                postfilter_gain = (int16_t)(3072 * (qg + 1));   // QCONST16(.09375f, 15)
+            }
+            tell = rd_tell(dec);
+        }
+        int isTransient;
+        if (LM > 0 && tell + 3 <= total_bits) {
+            isTransient = rd_bit_logp(dec, 3);
+            tell = rd_tell(dec);
+        } else {
+            isTransient = 0;
+        }
+        int intra_ener = tell + 3 <= total_bits ? rd_bit_logp(dec, 3) : 0;
+        if (!intra_ener && st->loss_duration != 0) energy_after_loss(st, start, end, LM);
+        PHASE_BEGIN(t_ce);
+        unquant_coarse_energy(start, end, oldBandE, intra_ener, dec, C, LM);
+        PHASE_END(PH_CELT_COARSE, t_ce, L.id);
+        tf_decode(start, end, isTransient, tf_res, LM, dec);
+        tell = rd_tell(dec);
+        int spread_decision = SPREAD_NORMAL;
+        if (tell + 4 <= total_bits) spread_decision = rd_icdf(dec, T_celt_spread_icdf, 5);
+        int32_t *cap = w->cap, *offsets = w->offsets;
+        init_caps(cap, LM, C);
+        int dynalloc_logp = 6;
+        total_bits <<= 3;
+        tell = (int32_t)rd_tell_frac(dec);
+        for (int i = start; i < end; i++) {
+            int width = C * (eB[i + 1] - eB[i]) << LM;
+            int quanta = imin(width << 3, imax(6 << 3, width));
+            int dll = dynalloc_logp, boost = 0;
+            while (tell + (dll << 3) < total_bits && boost < cap[i]) {
+                int flag = rd_bit_logp(dec, dll);
+                tell = (int32_t)rd_tell_frac(dec);
+                if (!flag) break;
+                boost += quanta;
+                total_bits -= quanta;
+                dll = 1;
+            }
+            offsets[i] = boost;
+            if (boost > 0) dynalloc_logp = imax(2, dynalloc_logp - 1);
+        }
+        int alloc_trim = tell + (6 << 3) <= total_bits ? rd_icdf(dec, T_celt_trim_icdf, 7) : 5;
+        int32_t bits = (((int32_t)len * 8) << 3) - (int32_t)rd_tell_frac(dec) - 1;
+        int anti_collapse_rsv = isTransient && LM >= 2 && bits >= ((LM + 2) << 3) ? (1 << 3) : 0;
+        bits -= anti_collapse_rsv;
+        int intensity = 0, dual_stereo = 0;
+        int32_t balance;
+        PHASE_BEGIN(t_al);
+        int codedBands = clt_compute_allocation(start, end, offsets, cap, alloc_trim, &intensity, &dual_stereo,
+                                                bits, &balance, pulses, fine_quant, fine_priority, C, LM, dec, w);
+        PHASE_END(PH_CELT_ALLOC, t_al, L.id);
+        unquant_fine_energy(start, end, oldBandE, fine_quant, dec, C);
+        hv[H_SILENCE] = silence;
+        hv[H_PF_GAIN] = postfilter_gain;
+        hv[H_PF_PITCH] = postfilter_pitch;
+        hv[H_PF_TAPSET] = postfilter_tapset;
+        hv[H_TRANSIENT] = isTransient;
+        hv[H_SPREAD] = spread_decision;
+        hv[H_AC_RSV] = anti_collapse_rsv;
+        hv[H_INTENSITY] = intensity;
+        hv[H_DUAL] = dual_stereo;
+        hv[H_BALANCE] = balance;
+        hv[H_CODED] = codedBands;
+    });
+    for (int k = 0; k < H_N; k++) hv[k] = lbcast(L, hv[k]);
+    const int silence = hv[H_SILENCE];
+    const int16_t postfilter_gain = (int16_t)hv[H_PF_GAIN];
+    const int postfilter_pitch = hv[H_PF_PITCH], postfilter_tapset = hv[H_PF_TAPSET];
+    const int isTransient = hv[H_TRANSIENT], shortBlocks = isTransient ? M : 0;
+    const int spread_decision = hv[H_SPREAD], anti_collapse_rsv = hv[H_AC_RSV];
+    const int intensity = hv[H_INTENSITY], dual_stereo = hv[H_DUAL];
+    const int32_t balance = hv[H_BALANCE];
+    const int codedBands = hv[H_CODED];
     PHASE_BEGIN(t_sh);
     for (int c = 0; c < CC; c++) lshift_copy(L, st->decode_mem[c], CELT_DEC_BUF - N + CELT_OVERLAP, N);
     PHASE_END(PH_CELT_SHIFT, t_sh, L.id);
     int16_t *X = w->X;
+    // The band shapes: the PVQ split recursion updates its stack, the band
+    // vectors and the folding buffer in place from entropy-decoded values,
+    // so it runs on the first lane as a group of one.
     PHASE_BEGIN(t_qb);
-    quant_all_bands_dec(L, start, end, X, C == 2 ? X + N : 0, w->collapse_masks, pulses, shortBlocks,
-                        spread_decision, dual_stereo, intensity, tf_res, len * (8 << 3) - anti_collapse_rsv,
-                        balance, dec, LM, codedBands, &st->rng, st->disable_inv, w);
+    lead_rd(L, dec, [&]() CUO_INLINE {
+        quant_all_bands_dec(lone(L), start, end, X, C == 2 ? X + N : 0, w->collapse_masks, pulses, shortBlocks,
+                            spread_decision, dual_stereo, intensity, tf_res, len * (8 << 3) - anti_collapse_rsv,
+                            balance, dec, LM, codedBands, &st->rng, st->disable_inv, w);
+    });
     PHASE_END(PH_CELT_BANDS, t_qb, L.id);
     int anti_collapse_on = 0;
-    if (anti_collapse_rsv > 0) anti_collapse_on = (int)rd_bits(dec, 1);
-    unquant_energy_finalise(start, end, oldBandE, fine_quant, fine_priority, len * 8 - rd_tell(dec), dec, C);
-    if (anti_collapse_on)
-        anti_collapse(L, X, w->collapse_masks, LM, C, N, start, end, oldBandE, oldLogE, oldLogE2, pulses, st->rng);
-    if (silence)
-        for (int i = 0; i < C * CELT_NB; i++) oldBandE[i] = -28672;   // -QCONST16(28.f, DB_SHIFT)
-    if (st->prefilter_and_fold) prefilter_and_fold(st, N, w);
-    lsync(L);
+    lead_rd(L, dec, [&]() CUO_INLINE {
+        if (anti_collapse_rsv > 0) anti_collapse_on = (int)rd_bits(dec, 1);
+        unquant_energy_finalise(start, end, oldBandE, fine_quant, fine_priority, len * 8 - rd_tell(dec), dec, C);
+    });
+    anti_collapse_on = lbcast(L, anti_collapse_on);
+    lead(L, [&]() CUO_INLINE {
+        if (anti_collapse_on)
+            anti_collapse(lone(L), X, w->collapse_masks, LM, C, N, start, end, oldBandE, oldLogE, oldLogE2, pulses,
+                          st->rng);
+        if (silence)
+            for (int i = 0; i < C * CELT_NB; i++) oldBandE[i] = -28672;   // -QCONST16(28.f, DB_SHIFT)
+        if (st->prefilter_and_fold) prefilter_and_fold(st, N, w);
+    });
     PHASE_BEGIN(t_sy);
     celt_synthesis(L, w, X, out_syn, oldBandE, start, effEnd, C, CC, isTransient, LM, silence);
     PHASE_END(PH_CELT_SYNTH, t_sy, L.id);
     PHASE_BEGIN(t_cb);
+    // the post-filter state is read once into registers here and written back
+    // on the first lane after the filter, both with the period floored at 15
+    const int pf_period = imax(st->postfilter_period, 15), pf_period_old = imax(st->postfilter_period_old, 15);
+    const int16_t pf_gain = (int16_t)st->postfilter_gain, pf_gain_old = (int16_t)st->postfilter_gain_old;
+    const int pf_tapset = st->postfilter_tapset, pf_tapset_old = st->postfilter_tapset_old;
     for (int c = 0; c < CC; c++) {
-        st->postfilter_period = imax(st->postfilter_period, 15);
-        st->postfilter_period_old = imax(st->postfilter_period_old, 15);
-        comb_filter_lanes(L, out_syn[c], out_syn[c], st->postfilter_period_old, st->postfilter_period, T_CELT_SHORTMDCT,
-                    (int16_t)st->postfilter_gain_old, (int16_t)st->postfilter_gain, st->postfilter_tapset_old,
-                    st->postfilter_tapset, T_celt_window, CELT_OVERLAP);
+        comb_filter_lanes(L, out_syn[c], out_syn[c], pf_period_old, pf_period, T_CELT_SHORTMDCT, pf_gain_old,
+                          pf_gain, pf_tapset_old, pf_tapset, T_celt_window, CELT_OVERLAP);
         if (LM != 0)
-            comb_filter_lanes(L, out_syn[c] + T_CELT_SHORTMDCT, out_syn[c] + T_CELT_SHORTMDCT, st->postfilter_period,
-                        postfilter_pitch, N - T_CELT_SHORTMDCT, (int16_t)st->postfilter_gain, postfilter_gain,
-                        st->postfilter_tapset, postfilter_tapset, T_celt_window, CELT_OVERLAP);
+            comb_filter_lanes(L, out_syn[c] + T_CELT_SHORTMDCT, out_syn[c] + T_CELT_SHORTMDCT, pf_period,
+                              postfilter_pitch, N - T_CELT_SHORTMDCT, pf_gain, postfilter_gain, pf_tapset,
+                              postfilter_tapset, T_celt_window, CELT_OVERLAP);
     }
-    lsync(L);
     PHASE_END(PH_CELT_COMB, t_cb, L.id);
-    st->postfilter_period_old = st->postfilter_period;
-    st->postfilter_gain_old = st->postfilter_gain;
-    st->postfilter_tapset_old = st->postfilter_tapset;
-    st->postfilter_period = postfilter_pitch;
-    st->postfilter_gain = postfilter_gain;
-    st->postfilter_tapset = postfilter_tapset;
-    if (LM != 0) {
-        st->postfilter_period_old = st->postfilter_period;
-        st->postfilter_gain_old = st->postfilter_gain;
-        st->postfilter_tapset_old = st->postfilter_tapset;
-    }
+    lead(L, [&]() CUO_INLINE {
+        st->postfilter_period_old = pf_period;
+        st->postfilter_gain_old = pf_gain;
+        st->postfilter_tapset_old = pf_tapset;
+        st->postfilter_period = postfilter_pitch;
+        st->postfilter_gain = postfilter_gain;
+        st->postfilter_tapset = postfilter_tapset;
+        if (LM != 0) {
+            st->postfilter_period_old = st->postfilter_period;
+            st->postfilter_gain_old = st->postfilter_gain;
+            st->postfilter_tapset_old = st->postfilter_tapset;
+        }
+    });
     // energy history: every band of both channels on its own, so lanes split them
     if (C == 1) {
         LFOR(L, i, 0, CELT_NB) oldBandE[CELT_NB + i] = oldBandE[i];
@@ -2300,15 +2341,16 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
             oldLogE[j] = oldLogE2[j] = -28672;
         }
     }
-    lsync(L);
-    st->rng = dec->rng;
     PHASE_BEGIN(t_de);
     deemphasis(L, out_syn[0], out_syn[1], pcm, N, CC, st->preemph_memD, accum);
     PHASE_END(PH_CELT_DEEMPH, t_de, L.id);
-    st->loss_duration = 0;
-    st->prefilter_and_fold = 0;
+    lead(L, [&]() CUO_INLINE {
+        st->rng = dec->rng;
+        st->loss_duration = 0;
+        st->prefilter_and_fold = 0;
+        if (rd_tell(dec) <= 8 * len && dec->error) st->error = 1;
+    });
     if (rd_tell(dec) > 8 * len) return -3;   // OPUS_INTERNAL_ERROR
-    if (dec->error) st->error = 1;
     return frame_size;
 }
 

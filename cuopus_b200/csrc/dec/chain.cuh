@@ -52,11 +52,22 @@ DFN void stage_init(const Lanes &L, PacketStage &S, uint8_t *region)
     lsync(L);
 }
 
-// Bounded wait for the completion of buffer b's copy; false on timeout.
-DFN bool stage_wait(PacketStage &S, int b)
+DFN unsigned long long stage_clock_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for the completion of buffer b's copy; false on timeout.  The
+// limit is `polls` mbarrier.try_wait rounds and, when limit_ns > 0, also
+// limit_ns of the device's global timer (whichever ends first is not a
+// timeout: both must run out).
+DFN bool stage_wait(PacketStage &S, int b, int polls = 1 << 20, unsigned long long limit_ns = 0)
 {
     uint32_t addr = smem_u32(&S.bar[b]), par = (S.parity >> b) & 1u;
-    for (int it = 0; it < (1 << 20); it++) {
+    const unsigned long long t0 = limit_ns ? stage_clock_ns() : 0;
+    for (int it = 0;; it++) {
         uint32_t done;
         asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
                      " selp.u32 %0, 1, 0, p;\n}\n"
@@ -68,8 +79,8 @@ DFN bool stage_wait(PacketStage &S, int b)
             S.pending &= ~(1u << b);
             return true;
         }
+        if (it >= polls && (!limit_ns || stage_clock_ns() - t0 > limit_ns)) return false;
     }
-    return false;
 }
 
 // Start staging packet (src, n) into buffer b.  Returns false when the packet
@@ -115,12 +126,19 @@ DFN bool stage_ready(const Lanes &L, PacketStage &S, int b)
 }
 
 // Before the group's region is reused or the kernel returns: let every copy in
-// flight land (bounded).
+// flight land.  A copy is at most STAGE_BUF bytes from global memory and
+// lands within microseconds; the decode loop gives up on one after 2^20
+// polls and reads the packet in place, but here the group must not leave its
+// shared memory while the copy can still write it (a later block on the SM
+// could own those bytes), so the wait runs for at least one second of the
+// global timer as well.  A copy that has not landed by then means the memory
+// system has failed; the group returns regardless (its chains' results are
+// already written) rather than spin without end.
 DFN void stage_drain(const Lanes &L, PacketStage &S)
 {
     bool ok = true;
     for (int b = 0; b < 2; b++)
-        if (S.pending & (1u << b)) ok = stage_wait(S, b) && ok;
+        if (S.pending & (1u << b)) ok = stage_wait(S, b, 1 << 20, 1000000000ull) && ok;
     if (!__all_sync(L.mask, ok)) S.ok = 0;
 }
 #endif

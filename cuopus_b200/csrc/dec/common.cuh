@@ -44,19 +44,85 @@ namespace cuo {
 
 // ------------------------------------------------------------------ lanes
 
+#if defined(CUO_LANE_SIM) && !defined(__CUDACC__)
+// Lane-interleaving host build (test only, lanesim.cpp): every lane of a group
+// is a fiber of its own and the fibers switch at random points of the decoder
+// code, so an access to group memory that depends on the lanes running in
+// lockstep shows up as a wrong sample.  The lane primitives below become
+// barriers and exchanges between the fibers.
+struct LaneSim;
+void lanesim_sync(LaneSim *s, int id);
+int32_t lanesim_sum(LaneSim *s, int id, int32_t v);
+void lanesim_scan_affine(LaneSim *s, int id, uint32_t *a, uint32_t *b);
+void lanesim_bcast(LaneSim *s, int id, void *p, int bytes);
+#endif
+
 struct Lanes {
     int id;          // lane index inside the chain's group
     int n;           // group width
     unsigned mask;   // warp mask of the group
+#if defined(CUO_LANE_SIM) && !defined(__CUDACC__)
+    LaneSim *sim;    // the group's fibers (null: one lane)
+#endif
 };
 
 DFN void lsync(const Lanes &L)
 {
 #ifdef __CUDA_ARCH__
     __syncwarp(L.mask);
+#elif defined(CUO_LANE_SIM)
+    if (L.sim) lanesim_sync(L.sim, L.id);
 #else
     (void)L;
 #endif
+}
+
+// A serial stretch on the group's first lane alone; the other lanes wait at
+// the barrier after it.  Code that updates group memory in place (reads a
+// location, then writes it) is correct only if no lane writes a location that
+// another lane has yet to read, and nothing keeps the lanes of a group in
+// lockstep between barriers; with one lane doing all of the stretch's reads
+// and writes, and barriers on both sides, that holds by construction.  Values
+// the other lanes need afterwards go through group memory (or lbcast /
+// rd_bcast).
+// Lead bodies are written [&]() CUO_INLINE { ... }: inlined into the caller, so
+// the variables they share with it stay in registers.
+#define CUO_INLINE __attribute__((always_inline))
+template <class F> DFN void lead(const Lanes &L, F &&body)
+{
+    lsync(L);
+    if (L.id == 0) body();
+    lsync(L);
+}
+
+// This lane as a group of its own, for a lead stretch that calls lane-split
+// code: every LFOR iteration then runs on this lane and the barriers and
+// lane sums reduce to nothing.
+DFN Lanes lone(const Lanes &L)
+{
+    Lanes s = L;
+    s.id = 0;
+    s.n = 1;
+#ifdef __CUDA_ARCH__
+    s.mask = 1u << (threadIdx.x & 31);
+#endif
+#if defined(CUO_LANE_SIM) && !defined(__CUDACC__)
+    s.sim = nullptr;
+#endif
+    return s;
+}
+
+// The first lane's value of v, on every lane of the group.
+DFN int32_t lbcast(const Lanes &L, int32_t v)
+{
+#ifdef __CUDA_ARCH__
+    if (L.n > 1) v = __shfl_sync(L.mask, v, (int)(threadIdx.x & 31) - L.id);
+#elif defined(CUO_LANE_SIM)
+    if (L.sim) lanesim_bcast(L.sim, L.id, &v, (int)sizeof v);
+#else
+    (void)L;
+#endif
+    return v;
 }
 
 // for (i = start; i < end; i++) split across the lanes of the group.  The
@@ -99,6 +165,8 @@ DFN int32_t lsum(const Lanes &L, int32_t v)
 {
 #ifdef __CUDA_ARCH__
     for (int off = L.n >> 1; off > 0; off >>= 1) v = (int32_t)((uint32_t)v + (uint32_t)__shfl_xor_sync(L.mask, v, off));
+#elif defined(CUO_LANE_SIM)
+    if (L.sim) v = lanesim_sum(L.sim, L.id, v);
 #else
     (void)L;
 #endif
@@ -127,6 +195,13 @@ DFN void lscan_affine(const Lanes &L, uint32_t &a, uint32_t &b)
     } else {
         a = pa;
         b = pb;
+    }
+#elif defined(CUO_LANE_SIM)
+    if (L.sim) {
+        lanesim_scan_affine(L.sim, L.id, &a, &b);
+    } else {
+        a = 1;
+        b = 0;
     }
 #else
     (void)L;

@@ -246,20 +246,25 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
     frame_size = audiosize;
     int16_t *pcm_silk = w->pcm_silk[D];
 
+    // Every write of decoder state below happens in a lead stretch (first
+    // lane only, barriers on both sides), so that no lane changes a field
+    // another lane may still be reading.
     if (mode != MODE_CELT_ONLY) {
         int16_t *pcm_ptr = celt_accum ? pcm : pcm_silk;
-        if (st->prev_mode == MODE_CELT_ONLY) silk_reset_dec(&st->silk);
-        st->DecControl.payloadSize_ms = imax(10, 1000 * audiosize / 48000);
-        if (data != 0) {
-            st->DecControl.nChannelsInternal = st->stream_channels;
-            if (mode == MODE_SILK_ONLY) {
-                if (bandwidth == BW_NB) st->DecControl.internalSampleRate = 8000;
-                else if (bandwidth == BW_MB) st->DecControl.internalSampleRate = 12000;
-                else st->DecControl.internalSampleRate = 16000;
-            } else {
-                st->DecControl.internalSampleRate = 16000;
+        lead(L, [&]() CUO_INLINE {
+            if (st->prev_mode == MODE_CELT_ONLY) silk_reset_dec(&st->silk);
+            st->DecControl.payloadSize_ms = imax(10, 1000 * audiosize / 48000);
+            if (data != 0) {
+                st->DecControl.nChannelsInternal = st->stream_channels;
+                if (mode == MODE_SILK_ONLY) {
+                    if (bandwidth == BW_NB) st->DecControl.internalSampleRate = 8000;
+                    else if (bandwidth == BW_MB) st->DecControl.internalSampleRate = 12000;
+                    else st->DecControl.internalSampleRate = 16000;
+                } else {
+                    st->DecControl.internalSampleRate = 16000;
+                }
             }
-        }
+        });
         int lost_flag = data == 0 ? 1 : (fec ? 2 : 0);
         int decoded_samples = 0;
         do {
@@ -306,28 +311,38 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
             opus_frame<1>(L, st, 0, 0, pcm_transition, imin(F5, audiosize), w, 0);
         }
     }
-    if (bandwidth) {
-        int endband = 21;
-        switch (bandwidth) {
-        case BW_NB: endband = 13; break;
-        case BW_MB:
-        case BW_WB: endband = 17; break;
-        case BW_SWB: endband = 19; break;
-        default: endband = 21; break;
-        }
-        st->celt.end = endband;
-    }
-    st->celt.stream_channels = st->stream_channels;
     int16_t *redundant_audio = w->redundant_audio;
+    lead(L, [&]() CUO_INLINE {
+        if (bandwidth) {
+            int endband = 21;
+            switch (bandwidth) {
+            case BW_NB: endband = 13; break;
+            case BW_MB:
+            case BW_WB: endband = 17; break;
+            case BW_SWB: endband = 19; break;
+            default: endband = 21; break;
+            }
+            st->celt.end = endband;
+        }
+        st->celt.stream_channels = st->stream_channels;
+        if (redundancy && celt_to_silk) st->celt.start = 0;
+    });
     if (redundancy && celt_to_silk) {
-        st->celt.start = 0;
         celt_decode(L, &st->celt, data + len, redundancy_bytes, redundant_audio, F5, 0, 0, &w->celt);
         redundant_rng = st->celt.rng;
     }
-    st->celt.start = start_band;
+    // the previous mode decides the CELT reset and the hybrid -> SILK silence
+    // frame: read before the lead stretch that may change the CELT state
+    const int prev_mode = st->prev_mode, prev_redundancy = st->prev_redundancy;
+    const int silence_frame =
+        mode == MODE_SILK_ONLY && prev_mode == MODE_HYBRID && !(redundancy && celt_to_silk && prev_redundancy);
+    lead(L, [&]() CUO_INLINE {
+        st->celt.start = start_band;
+        if (mode != MODE_SILK_ONLY && mode != prev_mode && prev_mode > 0 && !prev_redundancy) celt_reset(&st->celt);
+        if (silence_frame) st->celt.start = 0;
+    });
     if (mode != MODE_SILK_ONLY) {
         int celt_frame_size = imin(F20, frame_size);
-        if (mode != st->prev_mode && st->prev_mode > 0 && !st->prev_redundancy) celt_reset(&st->celt);
         celt_ret = celt_decode(L, &st->celt, fec ? 0 : data, len, pcm, celt_frame_size, (data && !fec) ? &dec : 0,
                                celt_accum,
                                &w->celt);
@@ -337,24 +352,23 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
             LFOR(L, i, 0, frame_size * C) pcm[i] = 0;
             lsync(L);
         }
-        if (st->prev_mode == MODE_HYBRID && !(redundancy && celt_to_silk && st->prev_redundancy)) {
-            st->celt.start = 0;
-            celt_decode(L, &st->celt, silence, 2, pcm, F2_5, 0, celt_accum, &w->celt);
-        }
+        if (silence_frame) celt_decode(L, &st->celt, silence, 2, pcm, F2_5, 0, celt_accum, &w->celt);
     }
     if (mode != MODE_CELT_ONLY && !celt_accum) {
         LFOR(L, i, 0, frame_size * C) pcm[i] = c_sat16((int32_t)pcm[i] + pcm_silk[i]);
         lsync(L);
     }
     if (redundancy && !celt_to_silk) {
-        celt_reset(&st->celt);
-        st->celt.start = 0;
+        lead(L, [&]() CUO_INLINE {
+            celt_reset(&st->celt);
+            st->celt.start = 0;
+        });
         celt_decode(L, &st->celt, data + len, redundancy_bytes, redundant_audio, F5, 0, 0, &w->celt);
         redundant_rng = st->celt.rng;
         smooth_fade(L, pcm + C * (frame_size - F2_5), redundant_audio + C * F2_5, pcm + C * (frame_size - F2_5),
                     F2_5, C);
     }
-    if (redundancy && celt_to_silk && (st->prev_mode != MODE_SILK_ONLY || st->prev_redundancy)) {
+    if (redundancy && celt_to_silk && (prev_mode != MODE_SILK_ONLY || prev_redundancy)) {
         LFOR(L, i, 0, F2_5 * C) pcm[i] = redundant_audio[i];
         smooth_fade(L, redundant_audio + C * F2_5, pcm + C * F2_5, pcm + C * F2_5, F2_5, C);
     }
@@ -366,11 +380,12 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
             smooth_fade(L, pcm_transition, pcm, pcm, F2_5, C);
         }
     }
-    if (len <= 1) st->rangeFinal = 0;
-    else st->rangeFinal = dec.rng ^ redundant_rng;
-    st->prev_mode = mode;
-    st->prev_redundancy = redundancy && !celt_to_silk;
-    lsync(L);
+    lead(L, [&]() CUO_INLINE {
+        if (len <= 1) st->rangeFinal = 0;
+        else st->rangeFinal = dec.rng ^ redundant_rng;
+        st->prev_mode = mode;
+        st->prev_redundancy = redundancy && !celt_to_silk;
+    });
     return celt_ret < 0 ? celt_ret : audiosize;
 }
 
@@ -417,25 +432,27 @@ DNI int decode_fec(Lanes L, OpusDec *st, const uint8_t *data, int size0, int pac
     if (frame_size < packet_frame_size || packet_mode == MODE_CELT_ONLY || st->mode == MODE_CELT_ONLY) {
         int ret = conceal_samples(L, st, frame_size, frame_buf, w, emit);
         if (ret < 0) return ret;
-        st->last_packet_duration = ret;
+        lead(L, [&]() CUO_INLINE { st->last_packet_duration = ret; });
         return ret;
     }
     int duration_copy = st->last_packet_duration;
     if (frame_size - packet_frame_size != 0) {
         int ret = conceal_samples(L, st, frame_size - packet_frame_size, frame_buf, w, emit);
         if (ret < 0) {
-            st->last_packet_duration = duration_copy;
+            lead(L, [&]() CUO_INLINE { st->last_packet_duration = duration_copy; });
             return ret;
         }
     }
-    st->mode = packet_mode;
-    st->bandwidth = packet_bandwidth;
-    st->frame_size = packet_frame_size;
-    st->stream_channels = packet_stream_channels;
+    lead(L, [&]() CUO_INLINE {
+        st->mode = packet_mode;
+        st->bandwidth = packet_bandwidth;
+        st->frame_size = packet_frame_size;
+        st->stream_channels = packet_stream_channels;
+    });
     int ret = opus_frame<0>(L, st, data, size0, frame_buf, packet_frame_size, w, 1);
     if (ret < 0) return ret;
     emit(frame_buf, ret);
-    st->last_packet_duration = frame_size;
+    lead(L, [&]() CUO_INLINE { st->last_packet_duration = frame_size; });
     return frame_size;
 }
 
@@ -454,7 +471,7 @@ DFN int opus_decode_packet(Lanes L, OpusDec *st, const uint8_t *data, int32_t le
     if (len == 0 || data == 0) {
         int ret = conceal_samples(L, st, frame_size, frame_buf, w, emit);
         if (ret < 0) return ret;
-        st->last_packet_duration = ret;
+        lead(L, [&]() CUO_INLINE { st->last_packet_duration = ret; });
         return ret;
     }
     if (len < 0) return OPUS_BAD_ARG;
@@ -471,10 +488,12 @@ DFN int opus_decode_packet(Lanes L, OpusDec *st, const uint8_t *data, int32_t le
         return decode_fec(L, st, data, size[0], packet_mode, packet_bandwidth, packet_frame_size,
                           packet_stream_channels, frame_buf, w, emit);
     if (count * packet_frame_size > frame_size) return OPUS_BUFFER_TOO_SMALL;
-    st->mode = packet_mode;
-    st->bandwidth = packet_bandwidth;
-    st->frame_size = packet_frame_size;
-    st->stream_channels = packet_stream_channels;
+    lead(L, [&]() CUO_INLINE {
+        st->mode = packet_mode;
+        st->bandwidth = packet_bandwidth;
+        st->frame_size = packet_frame_size;
+        st->stream_channels = packet_stream_channels;
+    });
     int nb_samples = 0;
     for (int i = 0; i < count; i++) {
         int ret = opus_frame<0>(L, st, data, size[i], frame_buf, frame_size - nb_samples, w, 0);
@@ -483,7 +502,7 @@ DFN int opus_decode_packet(Lanes L, OpusDec *st, const uint8_t *data, int32_t le
         data += size[i];
         nb_samples += ret;
     }
-    st->last_packet_duration = nb_samples;
+    lead(L, [&]() CUO_INLINE { st->last_packet_duration = nb_samples; });
     return nb_samples;
 }
 

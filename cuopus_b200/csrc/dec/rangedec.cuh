@@ -28,6 +28,40 @@ struct RangeDec {
     int error;
 };
 
+// The first lane's decoder state on every lane of the group, after a lead
+// stretch (common.cuh) decoded symbols on the first lane only.  buf and
+// storage are the same on every lane already.
+DFN void rd_bcast(const Lanes &L, RangeDec *d)
+{
+#ifdef __CUDA_ARCH__
+    if (L.n == 1) return;
+    const int src = (int)(threadIdx.x & 31) - L.id;
+    d->end_offs = __shfl_sync(L.mask, d->end_offs, src);
+    d->end_window = __shfl_sync(L.mask, d->end_window, src);
+    d->nend_bits = __shfl_sync(L.mask, d->nend_bits, src);
+    d->nbits_total = __shfl_sync(L.mask, d->nbits_total, src);
+    d->offs = __shfl_sync(L.mask, d->offs, src);
+    d->rng = __shfl_sync(L.mask, d->rng, src);
+    d->val = __shfl_sync(L.mask, d->val, src);
+    d->ext = __shfl_sync(L.mask, d->ext, src);
+    d->rem = __shfl_sync(L.mask, d->rem, src);
+    d->error = __shfl_sync(L.mask, d->error, src);
+#elif defined(CUO_LANE_SIM)
+    if (L.sim) lanesim_bcast(L.sim, L.id, d, (int)sizeof *d);
+#else
+    (void)L;
+    (void)d;
+#endif
+}
+
+// A lead stretch that decodes symbols: the body runs on the first lane, then
+// every lane continues from that lane's decoder state.
+template <class F> DFN void lead_rd(const Lanes &L, RangeDec *rd, F &&body)
+{
+    lead(L, body);
+    rd_bcast(L, rd);
+}
+
 DFN int rd_read_byte(RangeDec *d) { return d->offs < d->storage ? d->buf[d->offs++] : 0; }
 DFN int rd_read_byte_end(RangeDec *d)
 {

@@ -908,7 +908,10 @@ DNI void silk_decode_core(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *xq, con
         }
         lsync(L);
     }
-    // LPC synthesis history: the last 16 outputs, in registers (win[15] newest)
+    // LPC synthesis history: the last 16 outputs, in registers (win[15] newest);
+    // the previous subframe's gain, also in a register: both are written back
+    // after the frame's last barrier
+    int32_t prev_gain_Q16 = c->prev_gain_Q16;
     int32_t win[16];
 #pragma unroll
     for (int t = 0; t < 16; t++) win[t] = c->sLPC_Q14_buf[t];
@@ -926,14 +929,14 @@ DNI void silk_decode_core(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *xq, con
         int32_t Gain_Q10 = ctrl->Gains_Q16[k] >> 6;
         int32_t inv_gain_Q31 = s_inverse32_varq(ctrl->Gains_Q16[k], 47);
         int32_t gain_adj_Q16;
-        if (ctrl->Gains_Q16[k] != c->prev_gain_Q16) {
-            gain_adj_Q16 = s_div32_varq(c->prev_gain_Q16, ctrl->Gains_Q16[k], 16);
+        if (ctrl->Gains_Q16[k] != prev_gain_Q16) {
+            gain_adj_Q16 = s_div32_varq(prev_gain_Q16, ctrl->Gains_Q16[k], 16);
 #pragma unroll
             for (int t = 0; t < 16; t++) win[t] = s_smulww(gain_adj_Q16, win[t]);
         } else {
             gain_adj_Q16 = 1 << 16;
         }
-        c->prev_gain_Q16 = ctrl->Gains_Q16[k];
+        prev_gain_Q16 = ctrl->Gains_Q16[k];
         if (c->lossCnt && c->prevSignalType == SIG_VOICED && ix->signalType != SIG_VOICED && k < 2) {
             for (int i = 0; i < 5; i++) B_Q14[i] = 0;
             B_Q14[2] = 4096;   // SILK_FIX_CONST(0.25, 14)
@@ -1015,10 +1018,12 @@ DNI void silk_decode_core(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *xq, con
         }
         pexc += c->subfr_length;
         pxq += c->subfr_length;
+        lsync(L);   // the next subframe's LTP rewrites res_Q14, which this one's synthesis reads
     }
     lsync(L);
 #pragma unroll
     for (int t = 0; t < 16; t++) c->sLPC_Q14_buf[t] = win[t];
+    c->prev_gain_Q16 = prev_gain_Q16;
     lsync(L);
 }
 
@@ -1068,104 +1073,115 @@ DNI void silk_plc_conceal(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *frame, 
     SilkPLC *p = &c->sPLC;
     int32_t *sLTP_Q14 = w->sLTP_Q15;
     int16_t *sLTP = w->sLTP;
-    int32_t prevGain_Q10[2] = {p->prevGain_Q16[0] >> 6, p->prevGain_Q16[1] >> 6};
-    if (c->first_frame_after_reset) for (int i = 0; i < 16; i++) p->prevLPC_Q12[i] = 0;
-
-    // silk_PLC_energy
-    int32_t energy1, energy2;
-    int shift1, shift2;
-    {
-        int16_t *eb = w->plc_exc;
-        for (int k = 0; k < 2; k++)
-            for (int i = 0; i < c->subfr_length; i++)
-                eb[k * c->subfr_length + i] = (int16_t)s_sat16(s_smulww(
-                    c->exc_Q14[i + (k + c->nb_subfr - 2) * c->subfr_length], prevGain_Q10[k]) >> 8);
-        silk_sum_sqr_shift(&energy1, &shift1, eb, c->subfr_length);
-        silk_sum_sqr_shift(&energy2, &shift2, &eb[c->subfr_length], c->subfr_length);
-    }
-    const int32_t *rand_ptr;
-    if ((energy1 >> shift2) < (energy2 >> shift1))
-        rand_ptr = &c->exc_Q14[imax(0, (p->nb_subfr - 1) * p->subfr_length - 128)];
-    else
-        rand_ptr = &c->exc_Q14[imax(0, p->nb_subfr * p->subfr_length - 128)];
+    // The serial parts (energies, gains, the LPC chirp in place, the LTP
+    // excitation and the LPC synthesis) run on the first lane; the lanes split
+    // the LPC analysis filtering between them.  What the first lane computes
+    // for the second serial part stays in its registers.
+    int32_t prevGain_Q10[2] = {0, 0};
+    const int32_t *rand_ptr = nullptr;
     int16_t *B_Q14 = p->LTPCoef_Q14;
-    int16_t rand_scale_Q14 = p->randScale_Q14;
-    const int first_loss = c->lossCnt == 0;
-    int32_t harm_Gain_Q15 = first_loss ? 32440 : 31130;
-    int32_t rand_Gain_Q15 = c->prevSignalType == SIG_VOICED ? (first_loss ? 31130 : 26214)
-                                                            : (first_loss ? 32440 : 29491);
-    silk_bwexpander(p->prevLPC_Q12, c->LPC_order, 64881);   // SILK_FIX_CONST(0.99, 16)
+    int16_t rand_scale_Q14 = 0;
+    int32_t harm_Gain_Q15 = 0, rand_Gain_Q15 = 0;
+    lead(L, [&]() CUO_INLINE {
+        prevGain_Q10[0] = p->prevGain_Q16[0] >> 6;
+        prevGain_Q10[1] = p->prevGain_Q16[1] >> 6;
+        if (c->first_frame_after_reset) for (int i = 0; i < 16; i++) p->prevLPC_Q12[i] = 0;
+
+        // silk_PLC_energy
+        int32_t energy1, energy2;
+        int shift1, shift2;
+        {
+            int16_t *eb = w->plc_exc;
+            for (int k = 0; k < 2; k++)
+                for (int i = 0; i < c->subfr_length; i++)
+                    eb[k * c->subfr_length + i] = (int16_t)s_sat16(s_smulww(
+                        c->exc_Q14[i + (k + c->nb_subfr - 2) * c->subfr_length], prevGain_Q10[k]) >> 8);
+            silk_sum_sqr_shift(&energy1, &shift1, eb, c->subfr_length);
+            silk_sum_sqr_shift(&energy2, &shift2, &eb[c->subfr_length], c->subfr_length);
+        }
+        if ((energy1 >> shift2) < (energy2 >> shift1))
+            rand_ptr = &c->exc_Q14[imax(0, (p->nb_subfr - 1) * p->subfr_length - 128)];
+        else
+            rand_ptr = &c->exc_Q14[imax(0, p->nb_subfr * p->subfr_length - 128)];
+        rand_scale_Q14 = p->randScale_Q14;
+        const int first_loss = c->lossCnt == 0;
+        harm_Gain_Q15 = first_loss ? 32440 : 31130;
+        rand_Gain_Q15 = c->prevSignalType == SIG_VOICED ? (first_loss ? 31130 : 26214)
+                                                        : (first_loss ? 32440 : 29491);
+        silk_bwexpander(p->prevLPC_Q12, c->LPC_order, 64881);   // SILK_FIX_CONST(0.99, 16)
+        if (c->lossCnt == 0) {
+            rand_scale_Q14 = 1 << 14;
+            if (c->prevSignalType == SIG_VOICED) {
+                for (int i = 0; i < 5; i++) rand_scale_Q14 = (int16_t)(rand_scale_Q14 - B_Q14[i]);
+                rand_scale_Q14 = rand_scale_Q14 > 3277 ? rand_scale_Q14 : 3277;
+                rand_scale_Q14 = (int16_t)(s_smulbb(rand_scale_Q14, p->prevLTP_scale_Q14) >> 14);
+            } else {
+                int32_t invGain_Q30 = silk_lpc_inv_pred_gain(p->prevLPC_Q12, c->LPC_order, w->sw.A);
+                int32_t down = min32((1 << 30) >> 3, invGain_Q30);
+                down = max32((1 << 30) >> 8, down);
+                down = shl32(down, 3);
+                rand_Gain_Q15 = s_smulwb(down, rand_Gain_Q15) >> 14;
+            }
+        }
+    });
     int16_t A_Q12[16];
     for (int i = 0; i < c->LPC_order; i++) A_Q12[i] = p->prevLPC_Q12[i];
-    if (c->lossCnt == 0) {
-        rand_scale_Q14 = 1 << 14;
-        if (c->prevSignalType == SIG_VOICED) {
-            for (int i = 0; i < 5; i++) rand_scale_Q14 = (int16_t)(rand_scale_Q14 - B_Q14[i]);
-            rand_scale_Q14 = rand_scale_Q14 > 3277 ? rand_scale_Q14 : 3277;
-            rand_scale_Q14 = (int16_t)(s_smulbb(rand_scale_Q14, p->prevLTP_scale_Q14) >> 14);
-        } else {
-            int32_t invGain_Q30 = silk_lpc_inv_pred_gain(p->prevLPC_Q12, c->LPC_order, w->sw.A);
-            int32_t down = min32((1 << 30) >> 3, invGain_Q30);
-            down = max32((1 << 30) >> 8, down);
-            down = shl32(down, 3);
-            rand_Gain_Q15 = s_smulwb(down, rand_Gain_Q15) >> 14;
-        }
-    }
-    int32_t rand_seed = p->rand_seed;
     int lag = s_rshift_round(p->pitchL_Q8, 8);
-    int sLTP_buf_idx = c->ltp_mem_length;
     int idx = c->ltp_mem_length - lag - c->LPC_order - 2;
     silk_lpc_analysis_filter(L, &sLTP[idx], &c->outBuf[idx], A_Q12, c->ltp_mem_length - idx, c->LPC_order);
     int32_t inv_gain_Q30 = s_inverse32_varq(p->prevGain_Q16[1], 46);
     inv_gain_Q30 = min32(inv_gain_Q30, 0x7FFFFFFF >> 1);
     LFOR(L, i, idx + c->LPC_order, c->ltp_mem_length) sLTP_Q14[i] = s_smulwb(inv_gain_Q30, sLTP[i]);
-    lsync(L);
-    for (int k = 0; k < c->nb_subfr; k++) {
-        const int32_t *pl = &sLTP_Q14[sLTP_buf_idx - lag + 2];
-        for (int i = 0; i < c->subfr_length; i++) {
-            int32_t pr = 2;
-            pr = s_smlawb(pr, pl[i], B_Q14[0]);
-            pr = s_smlawb(pr, pl[i - 1], B_Q14[1]);
-            pr = s_smlawb(pr, pl[i - 2], B_Q14[2]);
-            pr = s_smlawb(pr, pl[i - 3], B_Q14[3]);
-            pr = s_smlawb(pr, pl[i - 4], B_Q14[4]);
-            rand_seed = s_rand(rand_seed);
-            int ri = (rand_seed >> 25) & 127;
-            sLTP_Q14[sLTP_buf_idx] = shl32(s_smlawb(pr, rand_ptr[ri], rand_scale_Q14), 2);
-            sLTP_buf_idx++;
+    lead(L, [&]() CUO_INLINE {
+        int32_t rand_seed = p->rand_seed;
+        int sLTP_buf_idx = c->ltp_mem_length;
+        for (int k = 0; k < c->nb_subfr; k++) {
+            const int32_t *pl = &sLTP_Q14[sLTP_buf_idx - lag + 2];
+            for (int i = 0; i < c->subfr_length; i++) {
+                int32_t pr = 2;
+                pr = s_smlawb(pr, pl[i], B_Q14[0]);
+                pr = s_smlawb(pr, pl[i - 1], B_Q14[1]);
+                pr = s_smlawb(pr, pl[i - 2], B_Q14[2]);
+                pr = s_smlawb(pr, pl[i - 3], B_Q14[3]);
+                pr = s_smlawb(pr, pl[i - 4], B_Q14[4]);
+                rand_seed = s_rand(rand_seed);
+                int ri = (rand_seed >> 25) & 127;
+                sLTP_Q14[sLTP_buf_idx] = shl32(s_smlawb(pr, rand_ptr[ri], rand_scale_Q14), 2);
+                sLTP_buf_idx++;
+            }
+            for (int j = 0; j < 5; j++) B_Q14[j] = (int16_t)(s_smulbb(harm_Gain_Q15, B_Q14[j]) >> 15);
+            rand_scale_Q14 = (int16_t)(s_smulbb(rand_scale_Q14, rand_Gain_Q15) >> 15);
+            p->pitchL_Q8 = s_smlawb(p->pitchL_Q8, p->pitchL_Q8, 655);
+            p->pitchL_Q8 = min32(p->pitchL_Q8, shl32(s_smulbb(18, c->fs_kHz), 8));
+            lag = s_rshift_round(p->pitchL_Q8, 8);
         }
-        for (int j = 0; j < 5; j++) B_Q14[j] = (int16_t)(s_smulbb(harm_Gain_Q15, B_Q14[j]) >> 15);
-        rand_scale_Q14 = (int16_t)(s_smulbb(rand_scale_Q14, rand_Gain_Q15) >> 15);
-        p->pitchL_Q8 = s_smlawb(p->pitchL_Q8, p->pitchL_Q8, 655);
-        p->pitchL_Q8 = min32(p->pitchL_Q8, shl32(s_smulbb(18, c->fs_kHz), 8));
-        lag = s_rshift_round(p->pitchL_Q8, 8);
-    }
-    int32_t *sl = &sLTP_Q14[c->ltp_mem_length - 16];
-    for (int i = 0; i < 16; i++) sl[i] = c->sLPC_Q14_buf[i];
-    for (int i = 0; i < c->frame_length; i++) {
-        int32_t pr = c->LPC_order >> 1;
-        for (int j = 0; j < c->LPC_order; j++) pr = s_smlawb(pr, sl[16 + i - j - 1], A_Q12[j]);
-        sl[16 + i] = s_add_sat32(sl[16 + i], s_lshift_sat32(pr, 4));
-        frame[i] = (int16_t)s_sat16(s_sat16(s_rshift_round(s_smulww(sl[16 + i], prevGain_Q10[1]), 8)));
-    }
-    for (int i = 0; i < 16; i++) c->sLPC_Q14_buf[i] = sl[c->frame_length + i];
-    p->rand_seed = rand_seed;
-    p->randScale_Q14 = rand_scale_Q14;
-    for (int i = 0; i < 4; i++) ctrl->pitchL[i] = lag;
-    lsync(L);
+        int32_t *sl = &sLTP_Q14[c->ltp_mem_length - 16];
+        for (int i = 0; i < 16; i++) sl[i] = c->sLPC_Q14_buf[i];
+        for (int i = 0; i < c->frame_length; i++) {
+            int32_t pr = c->LPC_order >> 1;
+            for (int j = 0; j < c->LPC_order; j++) pr = s_smlawb(pr, sl[16 + i - j - 1], A_Q12[j]);
+            sl[16 + i] = s_add_sat32(sl[16 + i], s_lshift_sat32(pr, 4));
+            frame[i] = (int16_t)s_sat16(s_sat16(s_rshift_round(s_smulww(sl[16 + i], prevGain_Q10[1]), 8)));
+        }
+        for (int i = 0; i < 16; i++) c->sLPC_Q14_buf[i] = sl[c->frame_length + i];
+        p->rand_seed = rand_seed;
+        p->randScale_Q14 = rand_scale_Q14;
+        for (int i = 0; i < 4; i++) ctrl->pitchL[i] = lag;
+    });
 }
 
 DNI void silk_plc(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *frame, int lost, SilkScratch *w)
 {
-    if (c->fs_kHz != c->sPLC.fs_kHz) {
-        silk_plc_reset(c);
-        c->sPLC.fs_kHz = c->fs_kHz;
-    }
+    lead(L, [&]() CUO_INLINE {
+        if (c->fs_kHz != c->sPLC.fs_kHz) {
+            silk_plc_reset(c);
+            c->sPLC.fs_kHz = c->fs_kHz;
+        }
+        if (!lost) silk_plc_update(c, ctrl);
+    });
     if (lost) {
         silk_plc_conceal(L, c, ctrl, frame, w);
-        c->lossCnt++;
-    } else {
-        silk_plc_update(c, ctrl);
+        lead(L, [&]() CUO_INLINE { c->lossCnt++; });
     }
 }
 
@@ -1246,14 +1262,19 @@ DNI void silk_cng_generate(SilkChan *c, int16_t *frame, int length, SilkScratch 
 DNI void silk_cng(Lanes L, SilkChan *c, const SilkCtrl *ctrl, int16_t *frame, int length, SilkScratch *w)
 {
     SilkCNG *g = &c->sCNG;
-    if (c->fs_kHz != g->fs_kHz) {
-        silk_cng_reset(c);
-        g->fs_kHz = c->fs_kHz;
-    }
+    // state updates in place on the first lane; the lanes split the
+    // excitation history move
+    lead(L, [&]() CUO_INLINE {
+        if (c->fs_kHz != g->fs_kHz) {
+            silk_cng_reset(c);
+            g->fs_kHz = c->fs_kHz;
+        }
+        if (c->lossCnt == 0 && c->prevSignalType == SIG_NO_VOICE)
+            for (int i = 0; i < c->LPC_order; i++)
+                g->CNG_smth_NLSF_Q15[i] = (int16_t)(g->CNG_smth_NLSF_Q15[i] +
+                    s_smulwb((int32_t)c->prevNLSF_Q15[i] - (int32_t)g->CNG_smth_NLSF_Q15[i], 16348));
+    });
     if (c->lossCnt == 0 && c->prevSignalType == SIG_NO_VOICE) {
-        for (int i = 0; i < c->LPC_order; i++)
-            g->CNG_smth_NLSF_Q15[i] = (int16_t)(g->CNG_smth_NLSF_Q15[i] +
-                s_smulwb((int32_t)c->prevNLSF_Q15[i] - (int32_t)g->CNG_smth_NLSF_Q15[i], 16348));
         int32_t max_Gain_Q16 = 0;
         int subfr = 0;
         for (int i = 0; i < c->nb_subfr; i++)
@@ -1267,16 +1288,19 @@ DNI void silk_cng(Lanes L, SilkChan *c, const SilkCtrl *ctrl, int16_t *frame, in
             lsync(L);
         }
         LFOR(L, i, 0, S) g->CNG_exc_buf_Q14[i] = c->exc_Q14[subfr * S + i];
-        lsync(L);
-        for (int i = 0; i < c->nb_subfr; i++) {
-            g->CNG_smth_Gain_Q16 += s_smulwb(ctrl->Gains_Q16[i] - g->CNG_smth_Gain_Q16, 4634);
-            if (s_smulww(g->CNG_smth_Gain_Q16, 46396) > ctrl->Gains_Q16[i])
-                g->CNG_smth_Gain_Q16 = ctrl->Gains_Q16[i];
-        }
+        lead(L, [&]() CUO_INLINE {
+            for (int i = 0; i < c->nb_subfr; i++) {
+                g->CNG_smth_Gain_Q16 += s_smulwb(ctrl->Gains_Q16[i] - g->CNG_smth_Gain_Q16, 4634);
+                if (s_smulww(g->CNG_smth_Gain_Q16, 46396) > ctrl->Gains_Q16[i])
+                    g->CNG_smth_Gain_Q16 = ctrl->Gains_Q16[i];
+            }
+        });
     }
-    if (c->lossCnt) silk_cng_generate(c, frame, length, w);
-    else
-        for (int i = 0; i < c->LPC_order; i++) g->CNG_synth_state[i] = 0;
+    lead(L, [&]() CUO_INLINE {
+        if (c->lossCnt) silk_cng_generate(c, frame, length, w);
+        else
+            for (int i = 0; i < c->LPC_order; i++) g->CNG_synth_state[i] = 0;
+    });
 }
 
 // ------------------------------------------------------------------ frame
@@ -1287,19 +1311,23 @@ DNI void silk_decode_frame(Lanes L, SilkChan *c, RangeDec *rd, int16_t *pOut, in
 {
     SilkCtrl *ctrl = &w->ctrl;
     int Lf = c->frame_length;
-    ctrl->LTP_scale_Q14 = 0;
     if (lostFlag == LOSS_NONE || (lostFlag == LOSS_LBRR && c->LBRR_flags[c->nFramesDecoded] == 1)) {
         int16_t *pulses = w->pulses;
-        PHASE_BEGIN(t_ix);
-        silk_decode_indices(c, rd, c->nFramesDecoded, lostFlag, condCoding, &w->sw);
-        PHASE_END(PH_SILK_INDICES, t_ix, L.id);
-        PHASE_BEGIN(t_pu);
-        silk_decode_pulses(rd, pulses, c->indices.signalType, c->indices.quantOffsetType, c->frame_length,
-                           &w->sw);
-        PHASE_END(PH_SILK_PULSES, t_pu, L.id);
-        PHASE_BEGIN(t_pa);
-        silk_decode_parameters(c, ctrl, condCoding, &w->sw);
-        PHASE_END(PH_SILK_PARAMS, t_pa, L.id);
+        // side information, pulses and parameters: entropy decoding and
+        // state updates in place, on the first lane
+        lead_rd(L, rd, [&]() CUO_INLINE {
+            ctrl->LTP_scale_Q14 = 0;
+            PHASE_BEGIN(t_ix);
+            silk_decode_indices(c, rd, c->nFramesDecoded, lostFlag, condCoding, &w->sw);
+            PHASE_END(PH_SILK_INDICES, t_ix, L.id);
+            PHASE_BEGIN(t_pu);
+            silk_decode_pulses(rd, pulses, c->indices.signalType, c->indices.quantOffsetType, c->frame_length,
+                               &w->sw);
+            PHASE_END(PH_SILK_PULSES, t_pu, L.id);
+            PHASE_BEGIN(t_pa);
+            silk_decode_parameters(c, ctrl, condCoding, &w->sw);
+            PHASE_END(PH_SILK_PARAMS, t_pa, L.id);
+        });
         PHASE_BEGIN(t_co);
         silk_decode_core(L, c, ctrl, pOut, pulses, w);
         PHASE_END(PH_SILK_CORE, t_co, L.id);
@@ -1310,10 +1338,13 @@ DNI void silk_decode_frame(Lanes L, SilkChan *c, RangeDec *rd, int16_t *pOut, in
         PHASE_BEGIN(t_pl);
         silk_plc(L, c, ctrl, pOut, 0, w);
         PHASE_END(PH_SILK_PLC, t_pl, L.id);
-        c->lossCnt = 0;
-        c->prevSignalType = c->indices.signalType;
-        c->first_frame_after_reset = 0;
+        lead(L, [&]() CUO_INLINE {
+            c->lossCnt = 0;
+            c->prevSignalType = c->indices.signalType;
+            c->first_frame_after_reset = 0;
+        });
     } else {
+        lead(L, [&]() CUO_INLINE { ctrl->LTP_scale_Q14 = 0; });
         silk_plc(L, c, ctrl, pOut, 1, w);
         int mv = c->ltp_mem_length - c->frame_length;
         lshift_copy(L, c->outBuf, mv, c->frame_length);
@@ -1323,10 +1354,11 @@ DNI void silk_decode_frame(Lanes L, SilkChan *c, RangeDec *rd, int16_t *pOut, in
     PHASE_BEGIN(t_cn);
     silk_cng(L, c, ctrl, pOut, Lf, w);
     PHASE_END(PH_SILK_CNG, t_cn, L.id);
-    silk_plc_glue_frames(c, pOut, Lf);
-    c->lagPrev = ctrl->pitchL[c->nb_subfr - 1];
+    lead(L, [&]() CUO_INLINE {
+        silk_plc_glue_frames(c, pOut, Lf);
+        c->lagPrev = ctrl->pitchL[c->nb_subfr - 1];
+    });
     *pN = Lf;
-    lsync(L);
 }
 
 // silk/stereo_MS_to_LR.c; all samples depend only on inputs, so lanes split them
@@ -1395,90 +1427,104 @@ DNI int silk_skip_lbrr(SilkChan *cs, int nChannelsInternal, RangeDec *rd, int32_
 DNI int silk_decode(Lanes L, SilkDec *dec, SilkDecControl *ctl, int lostFlag, int newPacketFlag,
                     RangeDec *rd, int16_t *samplesOut, int32_t *nSamplesOut, SilkScratch *w)
 {
-    int decode_only_middle = 0, ret = 0;
+    int ret = 0;
     int32_t nSamplesOutDec = 0;
     int32_t MS_pred_Q13[2] = {0, 0};
     SilkChan *cs = dec->ch;
 
-    if (newPacketFlag)
-        for (int n = 0; n < ctl->nChannelsInternal; n++) cs[n].nFramesDecoded = 0;
-    if (ctl->nChannelsInternal > dec->nChannelsInternal) {
-        silk_reset_chan(&cs[1]);   // silk_init_decoder
-    }
-    int stereo_to_mono = ctl->nChannelsInternal == 1 && dec->nChannelsInternal == 2 &&
-                         ctl->internalSampleRate == 1000 * cs[0].fs_kHz;
-    if (cs[0].nFramesDecoded == 0) {
-        for (int n = 0; n < ctl->nChannelsInternal; n++) {
-            int ms = ctl->payloadSize_ms;
-            if (ms == 0 || ms == 10) { cs[n].nFramesPerPacket = 1; cs[n].nb_subfr = 2; }
-            else if (ms == 20) { cs[n].nFramesPerPacket = 1; cs[n].nb_subfr = 4; }
-            else if (ms == 40) { cs[n].nFramesPerPacket = 2; cs[n].nb_subfr = 4; }
-            else if (ms == 60) { cs[n].nFramesPerPacket = 3; cs[n].nb_subfr = 4; }
-            else return -203;   // SILK_DEC_INVALID_FRAME_SIZE
-            int fs_kHz_dec = (ctl->internalSampleRate >> 10) + 1;
-            if (fs_kHz_dec != 8 && fs_kHz_dec != 12 && fs_kHz_dec != 16) return -200;
-            silk_decoder_set_fs(&cs[n], fs_kHz_dec, ctl->API_sampleRate);
+    // The packet header: VAD and LBRR flags, skipped LBRR frames, stereo
+    // prediction, channel (re)configuration -- entropy decoding and state
+    // updates in place, on the first lane; every lane gets the outcome.
+    int hdr[6] = {0, 0, 0, 0, 0, 0};   // status, mid only, stereo to mono, MS pred 0 / 1, has side
+    lead_rd(L, rd, [&]() CUO_INLINE {
+    int32_t ms_pred[2] = {0, 0};
+        int decode_only_middle = 0;
+        if (newPacketFlag)
+            for (int n = 0; n < ctl->nChannelsInternal; n++) cs[n].nFramesDecoded = 0;
+        if (ctl->nChannelsInternal > dec->nChannelsInternal) {
+            silk_reset_chan(&cs[1]);   // silk_init_decoder
         }
-    }
-    if (ctl->nChannelsAPI == 2 && ctl->nChannelsInternal == 2 &&
-        (dec->nChannelsAPI == 1 || dec->nChannelsInternal == 1)) {
-        dec->sStereo.pred_prev_Q13[0] = dec->sStereo.pred_prev_Q13[1] = 0;
-        dec->sStereo.sSide[0] = dec->sStereo.sSide[1] = 0;
-        cs[1].resampler_state = cs[0].resampler_state;
-    }
-    dec->nChannelsAPI = ctl->nChannelsAPI;
-    dec->nChannelsInternal = ctl->nChannelsInternal;
-
-    if (lostFlag != LOSS_LOST && cs[0].nFramesDecoded == 0) {
-        for (int n = 0; n < ctl->nChannelsInternal; n++) {
-            for (int i = 0; i < cs[n].nFramesPerPacket; i++) cs[n].VAD_flags[i] = rd_bit_logp(rd, 1);
-            cs[n].LBRR_flag = rd_bit_logp(rd, 1);
-        }
-        for (int n = 0; n < ctl->nChannelsInternal; n++) {
-            cs[n].LBRR_flags[0] = cs[n].LBRR_flags[1] = cs[n].LBRR_flags[2] = 0;
-            if (cs[n].LBRR_flag) {
-                if (cs[n].nFramesPerPacket == 1) {
-                    cs[n].LBRR_flags[0] = 1;
-                } else {
-                    const uint8_t *t = cs[n].nFramesPerPacket == 2 ? T_silk_LBRR_flags_2_iCDF
-                                                                   : T_silk_LBRR_flags_3_iCDF;
-                    int sym = rd_icdf(rd, t, 8) + 1;
-                    for (int i = 0; i < cs[n].nFramesPerPacket; i++) cs[n].LBRR_flags[i] = (sym >> i) & 1;
-                }
+        hdr[2] = ctl->nChannelsInternal == 1 && dec->nChannelsInternal == 2 &&
+                             ctl->internalSampleRate == 1000 * cs[0].fs_kHz;
+        if (cs[0].nFramesDecoded == 0) {
+            for (int n = 0; n < ctl->nChannelsInternal; n++) {
+                int ms = ctl->payloadSize_ms;
+                if (ms == 0 || ms == 10) { cs[n].nFramesPerPacket = 1; cs[n].nb_subfr = 2; }
+                else if (ms == 20) { cs[n].nFramesPerPacket = 1; cs[n].nb_subfr = 4; }
+                else if (ms == 40) { cs[n].nFramesPerPacket = 2; cs[n].nb_subfr = 4; }
+                else if (ms == 60) { cs[n].nFramesPerPacket = 3; cs[n].nb_subfr = 4; }
+                else { hdr[0] = -203; return; }   // SILK_DEC_INVALID_FRAME_SIZE
+                int fs_kHz_dec = (ctl->internalSampleRate >> 10) + 1;
+                if (fs_kHz_dec != 8 && fs_kHz_dec != 12 && fs_kHz_dec != 16) { hdr[0] = -200; return; }
+                silk_decoder_set_fs(&cs[n], fs_kHz_dec, ctl->API_sampleRate);
             }
         }
-        if (lostFlag == LOSS_NONE && (cs[0].LBRR_flag || (ctl->nChannelsInternal == 2 && cs[1].LBRR_flag)))
-            decode_only_middle = silk_skip_lbrr(cs, ctl->nChannelsInternal, rd, MS_pred_Q13, decode_only_middle, w);
-    }
-    if (ctl->nChannelsInternal == 2) {
-        if (lostFlag == LOSS_NONE ||
-            (lostFlag == LOSS_LBRR && cs[0].LBRR_flags[cs[0].nFramesDecoded] == 1)) {
-            silk_stereo_decode_pred(rd, MS_pred_Q13);
-            if ((lostFlag == LOSS_NONE && cs[1].VAD_flags[cs[0].nFramesDecoded] == 0) ||
-                (lostFlag == LOSS_LBRR && cs[1].LBRR_flags[cs[0].nFramesDecoded] == 0))
-                decode_only_middle = rd_icdf(rd, T_silk_stereo_only_code_mid_iCDF, 8);
-            else
-                decode_only_middle = 0;
-        } else {
-            MS_pred_Q13[0] = dec->sStereo.pred_prev_Q13[0];
-            MS_pred_Q13[1] = dec->sStereo.pred_prev_Q13[1];
+        if (ctl->nChannelsAPI == 2 && ctl->nChannelsInternal == 2 &&
+            (dec->nChannelsAPI == 1 || dec->nChannelsInternal == 1)) {
+            dec->sStereo.pred_prev_Q13[0] = dec->sStereo.pred_prev_Q13[1] = 0;
+            dec->sStereo.sSide[0] = dec->sStereo.sSide[1] = 0;
+            cs[1].resampler_state = cs[0].resampler_state;
         }
-    }
-    if (ctl->nChannelsInternal == 2 && decode_only_middle == 0 && dec->prev_decode_only_middle == 1) {
-        memset(cs[1].outBuf, 0, sizeof(cs[1].outBuf));
-        memset(cs[1].sLPC_Q14_buf, 0, sizeof(cs[1].sLPC_Q14_buf));
-        cs[1].lagPrev = 100;
-        cs[1].LastGainIndex = 10;
-        cs[1].prevSignalType = SIG_NO_VOICE;
-        cs[1].first_frame_after_reset = 1;
-    }
+        dec->nChannelsAPI = ctl->nChannelsAPI;
+        dec->nChannelsInternal = ctl->nChannelsInternal;
+
+        if (lostFlag != LOSS_LOST && cs[0].nFramesDecoded == 0) {
+            for (int n = 0; n < ctl->nChannelsInternal; n++) {
+                for (int i = 0; i < cs[n].nFramesPerPacket; i++) cs[n].VAD_flags[i] = rd_bit_logp(rd, 1);
+                cs[n].LBRR_flag = rd_bit_logp(rd, 1);
+            }
+            for (int n = 0; n < ctl->nChannelsInternal; n++) {
+                cs[n].LBRR_flags[0] = cs[n].LBRR_flags[1] = cs[n].LBRR_flags[2] = 0;
+                if (cs[n].LBRR_flag) {
+                    if (cs[n].nFramesPerPacket == 1) {
+                        cs[n].LBRR_flags[0] = 1;
+                    } else {
+                        const uint8_t *t = cs[n].nFramesPerPacket == 2 ? T_silk_LBRR_flags_2_iCDF
+                                                                       : T_silk_LBRR_flags_3_iCDF;
+                        int sym = rd_icdf(rd, t, 8) + 1;
+                        for (int i = 0; i < cs[n].nFramesPerPacket; i++) cs[n].LBRR_flags[i] = (sym >> i) & 1;
+                    }
+                }
+            }
+            if (lostFlag == LOSS_NONE && (cs[0].LBRR_flag || (ctl->nChannelsInternal == 2 && cs[1].LBRR_flag)))
+                decode_only_middle = silk_skip_lbrr(cs, ctl->nChannelsInternal, rd, ms_pred, decode_only_middle, w);
+        }
+        if (ctl->nChannelsInternal == 2) {
+            if (lostFlag == LOSS_NONE ||
+                (lostFlag == LOSS_LBRR && cs[0].LBRR_flags[cs[0].nFramesDecoded] == 1)) {
+                silk_stereo_decode_pred(rd, ms_pred);
+                if ((lostFlag == LOSS_NONE && cs[1].VAD_flags[cs[0].nFramesDecoded] == 0) ||
+                    (lostFlag == LOSS_LBRR && cs[1].LBRR_flags[cs[0].nFramesDecoded] == 0))
+                    decode_only_middle = rd_icdf(rd, T_silk_stereo_only_code_mid_iCDF, 8);
+                else
+                    decode_only_middle = 0;
+            } else {
+                ms_pred[0] = dec->sStereo.pred_prev_Q13[0];
+                ms_pred[1] = dec->sStereo.pred_prev_Q13[1];
+            }
+        }
+        if (ctl->nChannelsInternal == 2 && decode_only_middle == 0 && dec->prev_decode_only_middle == 1) {
+            memset(cs[1].outBuf, 0, sizeof(cs[1].outBuf));
+            memset(cs[1].sLPC_Q14_buf, 0, sizeof(cs[1].sLPC_Q14_buf));
+            cs[1].lagPrev = 100;
+            cs[1].LastGainIndex = 10;
+            cs[1].prevSignalType = SIG_NO_VOICE;
+            cs[1].first_frame_after_reset = 1;
+        }
+        if (lostFlag == LOSS_NONE) hdr[5] = !decode_only_middle;
+        else hdr[5] = !dec->prev_decode_only_middle ||
+                        (ctl->nChannelsInternal == 2 && lostFlag == LOSS_LBRR &&
+                         cs[1].LBRR_flags[cs[1].nFramesDecoded] == 1);
+        hdr[1] = decode_only_middle;
+        hdr[3] = ms_pred[0];
+        hdr[4] = ms_pred[1];
+    });
+    for (int k = 0; k < 6; k++) hdr[k] = lbcast(L, hdr[k]);
+    if (hdr[0]) return hdr[0];
+    const int decode_only_middle = hdr[1], stereo_to_mono = hdr[2], has_side = hdr[5];
+    MS_pred_Q13[0] = hdr[3];
+    MS_pred_Q13[1] = hdr[4];
     int16_t *tmp[2] = {w->tmp[0], w->tmp[1]};
-    int has_side;
-    if (lostFlag == LOSS_NONE) has_side = !decode_only_middle;
-    else has_side = !dec->prev_decode_only_middle ||
-                    (ctl->nChannelsInternal == 2 && lostFlag == LOSS_LBRR &&
-                     cs[1].LBRR_flags[cs[1].nFramesDecoded] == 1);
-    lsync(L);
     for (int n = 0; n < ctl->nChannelsInternal; n++) {
         if (n == 0 || has_side) {
             int FrameIndex = cs[0].nFramesDecoded - n;
@@ -1492,9 +1538,8 @@ DNI int silk_decode(Lanes L, SilkDec *dec, SilkDecControl *ctl, int lostFlag, in
             nSamplesOutDec = nOut;
         } else {
             LFOR(L, i, 0, nSamplesOutDec) tmp[n][2 + i] = 0;
-            lsync(L);
         }
-        cs[n].nFramesDecoded++;
+        lead(L, [&]() CUO_INLINE { cs[n].nFramesDecoded++; });
     }
     if (ctl->nChannelsAPI == 2 && ctl->nChannelsInternal == 2) {
         PHASE_BEGIN(t_st);
@@ -1530,11 +1575,13 @@ DNI int silk_decode(Lanes L, SilkDec *dec, SilkDecControl *ctl, int lostFlag, in
         }
         lsync(L);
     }
-    if (lostFlag == LOSS_LOST) {
-        for (int i = 0; i < dec->nChannelsInternal; i++) cs[i].LastGainIndex = 10;
-    } else {
-        dec->prev_decode_only_middle = decode_only_middle;
-    }
+    lead(L, [&]() CUO_INLINE {
+        if (lostFlag == LOSS_LOST) {
+            for (int i = 0; i < dec->nChannelsInternal; i++) cs[i].LastGainIndex = 10;
+        } else {
+            dec->prev_decode_only_middle = decode_only_middle;
+        }
+    });
     return ret;
 }
 
