@@ -6,11 +6,12 @@
  * sources (FIXED_POINT) and prints every table from the compiled objects.
  * It is a one-off generator; its output, opus_tables.inc, is committed.
  *
- *   V=/root/reference/vendor/opus-1.5.2
- *   gcc -O0 -w -DOPUS_BUILD -DFIXED_POINT=1 -DUSE_ALLOCA -DHAVE_LRINT -DHAVE_LRINTF \
- *       -I$V/include -I$V/celt -I$V/silk -I$V/silk/fixed -I$V \
- *       gen_opus_tables.c -o /tmp/gen_opus_tables oracle/_ref/libopus_ref.so -lm && \
- *   LD_LIBRARY_PATH=oracle/_ref /tmp/gen_opus_tables > cuopus_b200/csrc/dec/opus_tables.inc
+ *   make -C oracle REF=<reference tree> tables
+ *
+ * builds it (oracle/_build/gen_opus_tables, linked with oracle/_ref's
+ * libopus) and rewrites cuopus_b200/csrc/dec/opus_tables.inc.  It lives
+ * beside the oracle because it compiles the reference's vendored sources; the
+ * product only includes its output.
  *
  * File-static tables (coarse-energy model, PVQ counts, log2 fractions, band
  * ordering) are reached by including the vendor translation units that own
