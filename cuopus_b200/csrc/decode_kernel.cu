@@ -16,6 +16,8 @@
 #define CUO_DECODE_KERNEL_TU 1
 #include <cuda_runtime.h>
 #include <stdio.h>
+
+#include <atomic>
 #include <string.h>
 
 #include "../../include/cuopus.h"
@@ -49,8 +51,10 @@ static __device__ __align__(256) unsigned char g_noalloc_slots[CUOPUS_NOALLOC_MA
 // Device address of g_noalloc_slots per device, looked up once with that
 // device current.  In host code the array's name is only a host-side stand-in
 // for the symbol, never a device address, so the kernel gets this pointer.
-static void *g_noalloc_ptr[64];
-static bool g_noalloc_ready[64];
+// Atomic so that first calls from several host threads (on one device or on
+// different ones) do not race on the lookup; a lookup done twice stores the
+// same address.
+static std::atomic<void *> g_noalloc_ptr[64];
 
 } // namespace cuo
 
@@ -63,24 +67,36 @@ static int noalloc_err(char *errbuf, size_t errcap, int rc, const char *msg, cud
     return rc;
 }
 
+extern "C" int cuopus_default_width(void);
+
 // The caller owns every table and output buffer (as in cuopus_decode_batch);
 // this entry point allocates nothing: decoder slots come from the static
 // array above, chains are dealt round-robin to at most
 // CUOPUS_NOALLOC_MAX_SLOTS resident groups, and no events, streams or graphs
-// are created.  Nothing in the slots needs clearing: a group initialises its
-// slot at the start of every chain and reads nothing it has not written.
+// are created.  Packets are staged in the launch's dynamic shared memory, as
+// in cuopus_decode_batch.  Nothing in the slots needs clearing: a group
+// initialises its slot at the start of every chain and reads nothing it has
+// not written.
 extern "C" int cuopus_decode_batch_noalloc(const cuopus_batch *b, void *cuda_stream, char *errbuf, size_t errcap)
 {
     using namespace cuo;
     if (errbuf && errcap) errbuf[0] = 0;
     if (!b) return noalloc_err(errbuf, errcap, 3, "batch is NULL", cudaSuccess);
     if (b->nchains <= 0) return 0;
-    int width = b->width > 0 ? b->width : 32;
+    int width = b->width > 0 ? b->width : cuopus_default_width();
     if (width != 1 && width != 2 && width != 4 && width != 8 && width != 16 && width != 32)
         return noalloc_err(errbuf, errcap, 3, "width is not a power of two <= 32", cudaSuccess);
-    int block = b->block > 0 ? b->block : 128;
+    int block = b->block;
+    if (block <= 0) {   // the largest block whose lane groups fit in the static slots
+        block = 0;
+        for (int cand = 128; cand >= 32 && !block; cand -= 32)
+            if (cand % width == 0 && cand / width <= CUOPUS_NOALLOC_MAX_SLOTS) block = cand;
+    }
     if ((block != 32 && block != 64 && block != 96 && block != 128) || block % width)
         return noalloc_err(errbuf, errcap, 3, "block must be 32, 64, 96 or 128 threads and a multiple of width",
+                           cudaSuccess);
+    if (block / width > CUOPUS_NOALLOC_MAX_SLOTS)
+        return noalloc_err(errbuf, errcap, 3, "block holds more lane groups than there are static decoder slots",
                            cudaSuccess);
     if (!b->data || !b->off || !b->len || !b->first || !b->npkts || !b->channels || !b->trim || !b->keep ||
         !b->res || (b->out && !b->out_off) || ((b->pkt_nsamp || b->pkt_rng) && !b->rec_off))
@@ -100,12 +116,11 @@ extern "C" int cuopus_decode_batch_noalloc(const cuopus_batch *b, void *cuda_str
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return noalloc_err(errbuf, errcap, 2, "cudaGetDevice", e);
     if (dev < 0 || dev >= 64) return noalloc_err(errbuf, errcap, 3, "device index out of range", cudaSuccess);
-    if (!g_noalloc_ready[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_slots);
+    void *slots = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+    if (!slots) {
+        e = cudaGetSymbolAddress(&slots, g_noalloc_slots);
         if (e != cudaSuccess) return noalloc_err(errbuf, errcap, 2, "cudaGetSymbolAddress of the decoder slots", e);
-        g_noalloc_ptr[dev] = p;
-        g_noalloc_ready[dev] = true;
+        g_noalloc_ptr[dev].store(slots, std::memory_order_release);
     }
     long long groups = b->nchains;
     long long cap = b->max_groups > 0 ? b->max_groups : CUOPUS_NOALLOC_MAX_SLOTS;
@@ -113,8 +128,6 @@ extern "C" int cuopus_decode_batch_noalloc(const cuopus_batch *b, void *cuda_str
     int gpb = block / width;
     int blocks = (int)((groups + gpb - 1) / gpb);
     if ((long long)blocks * gpb > CUOPUS_NOALLOC_MAX_SLOTS) blocks = CUOPUS_NOALLOC_MAX_SLOTS / gpb;
-    if (blocks < 1)
-        return noalloc_err(errbuf, errcap, 3, "block holds more groups than there are static slots", cudaSuccess);
     DecodeArgs a;
     memset(&a, 0, sizeof a);
     a.data = b->data;
@@ -132,14 +145,14 @@ extern "C" int cuopus_decode_batch_noalloc(const cuopus_batch *b, void *cuda_str
     a.pkt_nsamp = b->pkt_nsamp;
     a.pkt_rng = b->pkt_rng;
     a.res = (ChainResult *)b->res;
-    a.slots = (ChainSlot *)g_noalloc_ptr[dev];
+    a.slots = (ChainSlot *)slots;
     a.queue_head = nullptr;
     a.nchains = b->nchains;
     a.width = width;
     a.use_queue = 0;
+    a.scalar = b->scalar != 0;
     a.fec = b->fec != 0;
-    k_decode_chains<<<blocks, block, 0, st>>>(a);
-    e = cudaGetLastError();
+    e = decode_kernel_launch(a, blocks, block, st);
     if (e != cudaSuccess) return noalloc_err(errbuf, errcap, 2, "decode launch", e);
     e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return noalloc_err(errbuf, errcap, 2, "decode", e);

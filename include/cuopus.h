@@ -148,8 +148,14 @@ int cuopus_decode_batch(const cuopus_batch *b, void *cuda_stream, float *kernel_
  * the library allocates nothing: the decoder slots are a static device array
  * of CUOPUS_NOALLOC_MAX_SLOTS slots (about 4.9 MiB) that every GPU loading the
  * library holds until the process exits.  Chains are dealt round-robin to at
- * most that many lane groups (schedule, order and graph of *b are ignored);
- * max_groups above CUOPUS_NOALLOC_MAX_SLOTS is rejected with RC 3.  The first
+ * most that many lane groups; schedule, order, graph, light_sms and
+ * long_chains of *b are ignored (there is no queue counter to allocate),
+ * width, scalar and fec are honoured as in cuopus_decode_batch (width 0 =
+ * cuopus_default_width()), and block 0 picks the largest block whose lane
+ * groups fit in the slots (64 threads at width 1, 128 otherwise).
+ * max_groups above CUOPUS_NOALLOC_MAX_SLOTS, or a block holding more lane
+ * groups than that, is rejected with RC 3.  Packets are staged in shared
+ * memory as in cuopus_decode_batch.  The first
  * call on each device looks up the array's device address (with that device
  * current), so make that first call before any stream capture; the call
  * itself refuses to run during capture.  All calls share the one array:

@@ -7,9 +7,12 @@ workspace.
 
 Called through the C ABI and checked against cuopus_decode_batch on the same
 device tables: every chain's status, sample count, final range and every
-int16 sample must be identical, on two calls in a row (different batches, so
-the second call runs on slots the first one left behind).  This file is
-collected last on purpose."""
+int16 sample must be identical, on calls in a row (different batches, so
+each call runs on slots the previous one left behind).  Later cases make one
+lane group decode several chains in one call (max_groups = 3, and 141 chains
+on the 63 groups of 96-thread blocks), so a slot is also reused within a
+call, and one case leaves the block size to the entry point at one lane per
+chain.  This file is collected last on purpose."""
 import ctypes
 import os
 
@@ -50,9 +53,15 @@ def test_noalloc_matches_decode_batch_twice(cuda):
     lib.cuopus_decode_batch_noalloc.restype = ctypes.c_int
     lib.cuopus_decode_batch_noalloc.argtypes = [ctypes.POINTER(cn.Batch), ctypes.c_void_p, ctypes.c_char_p,
                                                 ctypes.c_size_t]
-    cases = [(["mixed_stereo_a", "mixed_mono_b", "long_hybrid"], 1.0, 32),
-             (["mixed_stereo_b", "plain_b", "code3_120ms", "short_stereo_300ms"], 0.5, 16)]
-    for names, seg, width in cases:
+    every = ["code3_120ms", "long_hybrid", "mixed_mono_a", "mixed_mono_b", "mixed_stereo_a", "mixed_stereo_b",
+             "one_packet", "plain_a", "plain_b", "short_100ms", "short_stereo_300ms"]
+    # (streams, seconds per chain, lanes per chain, block, max_groups)
+    cases = [(["mixed_stereo_a", "mixed_mono_b", "long_hybrid"], 1.0, 32, 0, 0),
+             (["mixed_stereo_b", "plain_b", "code3_120ms", "short_stereo_300ms"], 0.5, 16, 0, 0),
+             (every, 0.25, 32, 96, 0),
+             (["mixed_stereo_a", "mixed_mono_b", "long_hybrid"], 0.5, 8, 0, 3),
+             (["plain_b", "code3_120ms", "short_stereo_300ms"], 0.5, 1, 0, 0)]
+    for names, seg, width, block, max_groups in cases:
         pk, chs, nch = _tables(names, seg)
         b, keep_alive, meta = device_batch(pk, chs, nch)
         want = run_device_batch(b, meta, width=width, schedule=0)
@@ -60,7 +69,9 @@ def test_noalloc_matches_decode_batch_twice(cuda):
         assert np.all(want[:, 0] == 0)
         meta["T"]["out"].fill_(0x5A5A)
         meta["T"]["res"].fill_(-1)
-        b.width, b.block, b.schedule, b.max_groups = width, 0, 0, 0
+        if names is every:
+            assert meta["n"] > 64   # more chains than static slots: groups decode several each
+        b.width, b.block, b.schedule, b.max_groups = width, block, 0, max_groups
         rc, msg = _noalloc(lib, b)
         assert rc == 0, msg
         torch.cuda.synchronize()
