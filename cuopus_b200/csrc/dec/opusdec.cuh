@@ -166,6 +166,15 @@ DNI int packet_parse(const uint8_t *data, int32_t len, int16_t *size, int *paylo
     return count;
 }
 
+#ifdef CUO_FRAME_EVENTS
+// Defined by a test build: called once per decoded frame with the recursion
+// depth, the frame's mode, the previous mode, the redundancy flags, the
+// transition flag (5 ms concealment crossfade) and the hybrid -> SILK silence
+// frame flag.
+void cuo_frame_event(int depth, int mode, int prev_mode, int redundancy, int celt_to_silk, int transition,
+                     int silence_frame);
+#endif
+
 // src/opus_decoder.c smooth_fade (Fs 48 kHz: window increment 1)
 DNI void smooth_fade(Lanes L, const int16_t *in1, const int16_t *in2, int16_t *out, int overlap, int channels)
 {
@@ -380,6 +389,10 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
             smooth_fade(L, pcm_transition, pcm, pcm, F2_5, C);
         }
     }
+#ifdef CUO_FRAME_EVENTS
+    // test builds only: which branches of the frame decode ran
+    if (L.id == 0) cuo_frame_event(D, mode, prev_mode, redundancy, celt_to_silk, transition, silence_frame);
+#endif
     lead(L, [&]() CUO_INLINE {
         if (len <= 1) st->rangeFinal = 0;
         else st->rangeFinal = dec.rng ^ redundant_rng;

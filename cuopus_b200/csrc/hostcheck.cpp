@@ -8,7 +8,35 @@
 #include <stdlib.h>
 #include <string.h>
 
+#define CUO_FRAME_EVENTS 1
 #include "dec/chain.cuh"
+
+// Frame events of the host build (CUO_FRAME_EVENTS): counters the tests read
+// with hc_frame_events to show which branches of the frame decode their
+// streams exercise.  Index: 0 frames, 1 redundancy with celt_to_silk = 1,
+// 2 redundancy with celt_to_silk = 0, 3 transitions with the 5 ms crossfade,
+// 4 hybrid -> SILK silence frames, 5 concealment frames (depth 1),
+// 6 SILK -> CELT transitions, 7 CELT -> SILK/hybrid transitions.
+static unsigned long long g_events[8];
+static pthread_mutex_t g_events_mu = PTHREAD_MUTEX_INITIALIZER;
+
+void cuo::cuo_frame_event(int depth, int mode, int prev_mode, int redundancy, int celt_to_silk, int transition,
+                          int silence_frame)
+{
+    pthread_mutex_lock(&g_events_mu);
+    g_events[0]++;
+    if (redundancy && celt_to_silk) g_events[1]++;
+    if (redundancy && !celt_to_silk) g_events[2]++;
+    if (transition) {
+        g_events[3]++;
+        if (mode == 1002) g_events[6]++;
+        else g_events[7]++;
+    }
+    if (silence_frame) g_events[4]++;
+    if (depth > 0) g_events[5]++;
+    (void)prev_mode;
+    pthread_mutex_unlock(&g_events_mu);
+}
 
 extern "C" {
 
@@ -92,6 +120,17 @@ int hc_decode_chains(const uint8_t *data, const uint64_t *off, const uint32_t *l
 }
 
 unsigned long hc_slot_bytes(void) { return sizeof(cuo::ChainSlot); }
+
+// Copy the frame event counters (8 words, see cuo_frame_event) and reset them.
+void hc_frame_events(unsigned long long *out)
+{
+    pthread_mutex_lock(&g_events_mu);
+    for (int i = 0; i < 8; i++) {
+        out[i] = g_events[i];
+        g_events[i] = 0;
+    }
+    pthread_mutex_unlock(&g_events_mu);
+}
 
 }
 

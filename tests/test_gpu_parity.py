@@ -85,6 +85,21 @@ def test_mixed_whole_streams_many(cuda):
             _check([res[s]], pk[s], [(0, len(pk[s]), 0, res[s]["keep"])], nch[s], True)
 
 
+@pytest.mark.parametrize("channels,width", [(1, 32), (2, 32), (2, 4), (1, 1)])
+def test_spliced_mode_changes(cuda, channels, width):
+    """Mode changes without redundancy (CELT -> SILK / hybrid, SILK / hybrid ->
+    CELT, hybrid -> SILK with the CELT layer's silence frame): the 5 ms
+    concealment crossfades and silence frames of opus_decode_frame, bit-exact
+    (tests/branches.py builds the chains; test_branches.py shows they reach
+    those branches)."""
+    from branches import spliced_chains
+    from gpu_util import run_batch
+    packets, chains = spliced_chains(channels)
+    res, _ = run_batch([packets], [[(f, n, 0, 1 << 40) for f, n in chains]], [channels], width=width)
+    for i, (f, n) in enumerate(chains):
+        _check([res[i]], packets, [(f, n, 0, res[i]["keep"])], channels, True)
+
+
 def test_f16k_matches_cpu_pipeline(cuda):
     import torch
     from cuopus_b200 import cuopus_native as cn
