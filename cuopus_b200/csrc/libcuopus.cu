@@ -91,6 +91,7 @@ struct State {
     cuo::DecodeArgs g_args;
     float last_kernel_ms = 0.f;
     int last_ovf = 0;
+    int last_width = 0;                          // lanes per chain of the last file-entry decode
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;     // decode kernel
     cudaEvent_t evh0 = nullptr, evh1 = nullptr;   // packet / table upload
     cudaEvent_t evr0 = nullptr, evr1 = nullptr;   // resampler
@@ -561,6 +562,32 @@ int plan_files(const uint8_t *const *oggs, const size_t *ns, int nfiles, bool re
     return RC_OK;
 }
 
+// Lanes per chain of a file batch (CUOPUS_STRIDE, when set, decides).  A
+// batch's decode time is about max(longest chain, total work / decoder
+// groups) / per-group speed.  At 32 lanes a group decodes about 3x faster
+// than at 8 (lane-split loops), but 8 lanes give 6.4x the groups (every
+// resident group at 8 against 5 warps per SM at 32): long or uneven chains
+// (whole streams) decode faster at 32, many short chains (a long file cut in
+// 1 s chains) at 8.  Chain cost: its TOC samples x channels.
+int choose_width(const Plan &P)
+{
+    const char *e = getenv("CUOPUS_STRIDE");
+    if (e && atoi(e) > 0) return default_width();
+    double sum = 0.0, mx = 0.0;
+    for (size_t c = 0; c < P.first.size(); c++) {
+        double w = (double)P.cap[c] * (double)P.chans[c];
+        sum += w;
+        mx = std::max(mx, w);
+    }
+    long long g32 = default_max_groups(32);
+    if (g32 <= 0) g32 = resident_groups(BLOCK, 32);
+    long long g8 = resident_groups(BLOCK, 8);
+    const double speed32 = 3.0;   // per-group speed at 32 lanes relative to 8
+    double t32 = std::max(mx, sum / (double)std::max(g32, 1LL)) / speed32;
+    double t8 = std::max(mx, sum / (double)std::max(g8, 1LL));
+    return t8 < t32 ? 8 : 32;
+}
+
 // H2D of a plan, one decode launch into G.pcm, D2H of the results, validation.
 int run_plan(const Plan &P, cudaStream_t st, Err &err)
 {
@@ -618,9 +645,10 @@ int run_plan(const Plan &P, cudaStream_t st, Err &err)
     b.out = (int16_t *)G.pcm.p;
     b.res = (uint32_t *)G.res.p;
     b.nchains = (int32_t)nch;
-    b.width = default_width();
     if ((rc = ensure_occupancy(err))) return rc;
+    b.width = choose_width(P);
     b.max_groups = default_max_groups(b.width);
+    G.last_width = b.width;
     // longest chains first through the device queue: packets are the proxy
     std::vector<uint32_t> order(nch);
     std::iota(order.begin(), order.end(), 0u);
@@ -733,6 +761,7 @@ void record_stats(const Plan &P, bool resampled)
     if (cudaEventElapsedTime(&ms, G.ev0, G.ev1) == cudaSuccess) G.last.kernel_ms = ms;
     if (resampled && cudaEventElapsedTime(&ms, G.evr0, G.evr1) == cudaSuccess) G.last.resample_ms = ms;
     G.last.chains = (int64_t)P.first.size();
+    G.last.width = G.last_width;
     G.last.packets = (int64_t)P.len.size();
     int64_t play = 0;
     for (int64_t v : P.file_play48) play += v;

@@ -362,7 +362,7 @@ class Stats(ctypes.Structure):
     """cuopus_stats of include/cuopus.h."""
     _fields_ = [("demux_ms", ctypes.c_double), ("h2d_ms", ctypes.c_float), ("kernel_ms", ctypes.c_float),
                 ("resample_ms", ctypes.c_float), ("chains", ctypes.c_int64), ("packets", ctypes.c_int64),
-                ("play48", ctypes.c_int64)]
+                ("play48", ctypes.c_int64), ("width", ctypes.c_int32)]
 
 
 def last_stats():

@@ -289,12 +289,15 @@ typedef struct cuopus_stats {
     int64_t chains;
     int64_t packets;
     int64_t play48;
+    int32_t width;      /* lanes per chain the call decoded with */
 } cuopus_stats;
 
 int cuopus_last_stats(cuopus_stats *s);
 
 /* Extension: bytes of device state per decoder slot, and the number of lanes
- * per chain the entry points use (CUOPUS_STRIDE, default 32). */
+ * per chain cuopus_decode_batch uses when its width is 0 (CUOPUS_STRIDE,
+ * default 32).  The file entry points choose 32 or 8 lanes per call from the
+ * chains' lengths unless CUOPUS_STRIDE is set (cuopus_stats.width reports it). */
 long long cuopus_slot_bytes(void);
 int cuopus_default_width(void);
 
