@@ -49,10 +49,12 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     # name: (corpus kind, count, max seconds, chain segment seconds)
     "mixed4096": ("mixed", 4096, 30.0, 1e9),
+    # the cost model's training set for mixed4096: the same generator, other seeds
+    "mixed1024train": ("mixed", 1024, 30.0, 1e9),
     "pareto16384": ("pareto", 16384, 120.0, 1e9),
     "plain64": ("plain64", 64, 1.0, 1.0),
     "long7200": ("long", 1, 7200.0, 1.0),
-    "serve": ("lognormal", 512, 600.0, 1.0),
+    "serve": ("lognormal", 384, 7200.0, 1.0),
 }
 METRIC = "audio-sec decoded/sec on 1 B200 (bit-exact)"
 
@@ -63,13 +65,17 @@ def log(*a):
 
 # ------------------------------------------------------------------ inputs
 
+# the cost model trains on another corpus than the one it orders
+TRAIN_ON = {"mixed4096": "mixed1024train", "pareto16384": "mixed4096"}
+
+
 def load_inputs(workload, count=None):
     """Input preparation (never timed): generate or reuse the cached corpus."""
     from oracle.corpus import build_corpus
     kind, n, secs, seg = WORKLOADS[workload]
     t = time.time()
-    paths = build_corpus(kind, os.path.join(ROOT, "corpus"), count=count or n,
-                         seconds=secs if kind != "plain64" else None)
+    paths = build_corpus(kind, os.path.join(ROOT, "corpus"), seed=4321 if workload.endswith("train") else 1234,
+                         count=count or n, seconds=secs if kind != "plain64" else None)
     files = [open(p, "rb").read() for p in paths]
     log("corpus %s: %d files, %.1f MB, %.1fs" % (workload, len(files), sum(map(len, files)) / 1e6,
                                                  time.time() - t))
@@ -86,6 +92,7 @@ class DeviceBatch:
         base_b = 0
         base_p = 0
         self.audio_s = 0.0
+        self.file_play = []
         self.pkt_bytes = 0
         self.pcm_bytes = 0
         for f in files:
@@ -101,6 +108,7 @@ class DeviceBatch:
             base_b += len(ix.blob)
             base_p += len(ix.pkt_len)
             self.audio_s += ix.play48 / 48000.0
+            self.file_play.append(int(ix.play48) * ix.channels)
             self.pcm_bytes += int(ix.play48) * ix.channels * 2
             for c in range(len(ix.first)):   # packet bytes decoded, preroll packets included
                 a, b = int(ix.first[c]), int(ix.first[c]) + int(ix.npkts[c])
@@ -115,6 +123,10 @@ class DeviceBatch:
         self.chans = chans
         self.keep = keep
         tot = int((keep * chans.astype(np.uint64)).sum())
+        # host copies of the chain table: the full-size parity check after the
+        # timed region decodes every chain on the CPU from these
+        self.host = dict(blob=np.concatenate(blobs + [np.zeros(16, np.uint8)]), off=cat(offs), len=cat(lens),
+                         first=first, npkts=npk, chans=chans, trim=trim, keep=keep, out_off=out_off)
         dev = torch.device(device)
         T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
         self.t = dict(blob=T(np.concatenate(blobs + [np.zeros(16, np.uint8)])), off=T(cat(offs)),
@@ -230,6 +242,125 @@ def cpu_decode(files, seg, budget_s, threads):
     return audio / elapsed if elapsed > 0 else 0.0, audio, elapsed, used
 
 
+# ------------------------------------------------------------------ full-size parity
+
+def full_parity(db, threads, e2e_host):
+    """Untimed check of the timed batch's output after the timed region:
+    every chain decoded by libopus 1.5.2 fixed point on the host threads and
+    compared in place (every int16 sample of its keep window, its stop status,
+    sample count and final range: oref_check_chains).  The e2e output of the
+    last e2e step must equal the batch's PCM (int16), or the resampler oracle
+    over it with max abs diff 0 (f16k)."""
+    from oracle import ref_decode
+    t0 = time.time()
+    got = db.out.cpu().numpy()
+    res = db.results()
+    h = db.host
+    r = ref_decode.check_batch(h["blob"], h["off"], h["len"], h["first"], h["npkts"], h["chans"], h["trim"],
+                               h["keep"], got, h["out_off"], res, nthreads=threads)
+    fl = r["flags"]
+    out = {"oracle": "libopus 1.5.2 fixed point (oracle/_ref), fresh decoder per chain",
+           "chains_checked": int(db.n), "chains_total": int(db.n),
+           "pcm_mismatches": int(r["bad"].sum()), "chains_with_pcm_mismatch": int((r["bad"] > 0).sum()),
+           "range_mismatches": int(((fl & 4) != 0).sum()), "sample_count_mismatches": int(((fl & 2) != 0).sum()),
+           "stop_mismatches": int(((fl & 1) != 0).sum()), "samples_compared": int(got.size)}
+    if e2e_host is not None:
+        kind, buf, sizes = e2e_host
+        if kind == "i16":
+            hb = buf.numpy()[:got.size]
+            out["e2e_equals_batch"] = bool(hb.size == got.size and np.array_equal(hb, got))
+        else:
+            from oracle import pipeline
+            hb = buf.numpy()
+            o16 = o48 = 0
+            worst = 0.0
+            for f_i, n16 in enumerate(sizes):     # one file per f16k workload stream
+                n48 = int(db.file_play[f_i])
+                want = pipeline.resample(got[o48:o48 + n48], n16)
+                worst = max(worst, float(np.abs(hb[o16:o16 + n16] - want).max()) if n16 else 0.0)
+                o16 += n16
+                o48 += n48
+            out["e2e_f16k_max_abs_diff"] = worst
+    out["seconds"] = round(time.time() - t0, 1)
+    log("parity: %s" % json.dumps(out))
+    return out
+
+
+# ------------------------------------------------------------------ the reference's GPU library
+
+def reference_gpu_bench(args, files, seg):
+    """--impl reference-gpu: the reference's own libcuopus (built unchanged for
+    sm_100a by oracle/Makefile ref_gpu) against this library on the same GPU,
+    through the identical f16k call (cuopus_decode_f16k_multi, bound as the
+    reference's Python module binds it), on the workload's mono files (the
+    reference's GPU path is mono only), in groups of at most 2,048 chains of
+    1 s (the reference's one-launch limit).  Host Ogg bytes in, float32 16 kHz
+    in device memory out, stream synchronised: end-to-end time, K steps after
+    W warm-up steps, both libraries alternating step by step.  Outputs must
+    be identical."""
+    import ctypes
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from test_dropin import bind
+    from cuopus_b200 import cuopus_native as cn
+    ref_path = os.path.join(ROOT, "oracle", "_ref", "libcuopus_refgpu.so")
+    if not os.path.exists(ref_path):
+        return {"unavailable": "oracle/_ref/libcuopus_refgpu.so is not built (make -C oracle ref_gpu)"}
+    torch.cuda.set_device(0)
+    mono = [f for f in files if cn.probe_pcm(f)[1] == 1]
+    chains = [len(cn.index(f, seg_s=1.0).first) for f in mono]
+    groups, cur, cnt = [], [], 0
+    for f, c in zip(mono, chains):
+        if cur and cnt + c > 2048:
+            groups.append(cur)
+            cur, cnt = [], 0
+        cur.append(f)
+        cnt += c
+    if cur:
+        groups.append(cur)
+    audio = sum(cn.probe_pcm(f)[0] for f in mono) / 48000.0
+    stream = torch.cuda.current_stream()
+    libs = {"reference": bind(ref_path), "ours": bind(os.path.join(ROOT, "cuopus_b200", "lib", "libcuopus.so"))}
+    os.environ.setdefault("CUOPUS_SEG_S", "1")
+    n16s = [[cn.probe(f) for f in g] for g in groups]
+    outs = [[torch.empty(max(k, 1), dtype=torch.float32, device="cuda") for k in n] for n in n16s]
+    err = ctypes.create_string_buffer(512)
+
+    def step(lib):
+        for g, n16, o in zip(groups, n16s, outs):
+            n = len(g)
+            ba = (ctypes.c_char_p * n)(*g)
+            la = (ctypes.c_size_t * n)(*[len(f) for f in g])
+            oa = (ctypes.c_void_p * n)(*[t.data_ptr() for t in o])
+            ca = (ctypes.c_size_t * n)(*n16)
+            ol = (ctypes.c_int64 * n)()
+            rc = lib.cuopus_decode_f16k_multi(ba, la, n, oa, ca, ol, ctypes.c_void_p(stream.cuda_stream), err, 512)
+            if rc:
+                raise RuntimeError(err.value.decode())
+        torch.cuda.synchronize()
+
+    times = {k: [] for k in libs}
+    for i in range(args.warmup + args.steps):
+        for name, lib in libs.items():
+            t0 = time.perf_counter()
+            step(lib)
+            if i >= args.warmup:
+                times[name].append(time.perf_counter() - t0)
+    # the last step of each library: identical samples
+    same = True
+    keep = [[t.cpu().numpy() for t in o] for o in outs]
+    step(libs["reference"])
+    for o, k in zip(outs, keep):
+        for t, a in zip(o, k):
+            same = same and np.array_equal(t.cpu().numpy(), a)
+    med = {k: statistics.median(v) for k, v in times.items()}
+    return {"files": len(mono), "groups": len(groups), "chains": int(sum(chains)), "audio_s": round(audio, 1),
+            "reference": {"value": audio / med["reference"], "ms_per_step": med["reference"] * 1e3},
+            "ours": {"value": audio / med["ours"], "ms_per_step": med["ours"] * 1e3},
+            "speedup": med["reference"] / med["ours"], "identical_output": bool(same),
+            "call": "cuopus_decode_f16k_multi (reference binding), 1 s chains, 250 ms preroll"}
+
+
 # ------------------------------------------------------------------ helpers
 
 def peaks():
@@ -263,6 +394,80 @@ def timed_steps(cn, b, stream, steps):
     return e0.elapsed_time(e1) / steps, kern
 
 
+def train_cost_model(args, stream):
+    """The cost model of the scheduled form, trained (untimed) on another
+    corpus than the timed batch (TRAIN_ON): that corpus is decoded once with
+    the queue schedule in packet-count order, the decoder's per-chain decode
+    times are the targets, and the MLP is trained on the GPU."""
+    import torch
+    from cuopus_b200 import costmodel
+    from cuopus_b200 import cuopus_native as cn
+    name = TRAIN_ON.get(args.workload, "mixed1024train")
+    files, seg = load_inputs(name)
+    tb = DeviceBatch(files, seg, stream.device)
+    b = tb.batch(32, 1, costmodel.packet_order(tb.cap_pkts, tb.chans), 128, 0)
+    cn.decode_batch(b, stream.cuda_stream)
+    torch.cuda.synchronize()
+    times = np.maximum(tb.results()[:, 3].astype(np.float64), 1.0)
+    feats = costmodel.chain_features(b)
+    model = costmodel.CostModel(seed=1)
+    t0 = time.time()
+    losses = model.fit(feats, times, steps=1500, lr=3e-3)
+    train_s = time.time() - t0
+    y, yh = np.log(times), np.log(model.predict(feats))
+    r2 = 1.0 - np.sum((y - yh) ** 2) / np.sum((y - y.mean()) ** 2)
+    del tb, b, feats
+    torch.cuda.empty_cache()
+    return model, {"train_corpus": name, "train_chains": int(len(times)), "train_s": round(train_s, 2),
+                   "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
+                   "r2_log_time_train": round(float(r2), 4)}
+
+
+def compare_orders(cn, db, stream, b, info, reps=2):
+    """Untimed comparison of visiting orders on the timed batch with the
+    tuned launch: queue-schedule kernel time in learned and in packet-count
+    order, and each order's makespan as the scheduler predicts it (list
+    scheduling of the predicted, resp. packet-count-fitted, chain costs on the
+    launch's decoder groups) against the measured kernel time."""
+    import torch
+    from cuopus_b200 import costmodel
+    pred = info.pop("_pred", None)
+    out = {}
+    orders = {"packets": costmodel.packet_order(db.cap_pkts, db.chans)}
+    if pred is not None:
+        orders["learned"] = np.argsort(-pred, kind="stable")
+    keep = b.order
+    times = None
+    for name, order in orders.items():
+        arr = np.ascontiguousarray(order.astype(np.uint32))
+        b.order = arr.ctypes.data
+        ms = [cn.decode_batch(b, stream.cuda_stream) for _ in range(reps)]
+        torch.cuda.synchronize()
+        t = db.results()[:, 3].astype(np.float64)
+        times = t if times is None else times
+        out[name] = {"kernel_ms": float(min(ms))}
+    b.order = keep
+    groups = b.max_groups if b.max_groups > 0 else None
+    if groups is None:
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        groups = sms * 8 * (32 // b.width)
+    # per-chain costs in the unit of the measured chain times (us); the
+    # packet-count fallback predicts cost proportional to packets x channels,
+    # scaled to the measured total
+    w = db.cap_pkts.astype(np.float64) * db.chans.astype(np.float64)
+    pk_cost = w * (times.sum() / w.sum())
+    out["packets"]["predicted_ms"] = costmodel.makespan(pk_cost, orders["packets"], groups) / 1e3
+    if pred is not None:
+        lt = np.log(np.maximum(times, 1.0))
+        r2 = 1.0 - np.sum((lt - np.log(pred)) ** 2) / np.sum((lt - lt.mean()) ** 2)
+        out["learned"]["predicted_ms"] = costmodel.makespan(pred, orders["learned"], groups) / 1e3
+        out["r2_log_time_on_this_batch"] = round(float(r2), 4)
+        out["learned_over_packets"] = out["packets"]["kernel_ms"] / out["learned"]["kernel_ms"]
+    out["decoder_groups"] = int(groups)
+    out["longest_chain_ms"] = float(times.max() / 1e3)
+    return out
+
+
 def schedule_batch(cn, db, stream, args):
     """Warm-up work of the scheduled form (untimed): plain form timing, cycle
     recording, cost model training, autotuning.  Returns (batch, info)."""
@@ -285,23 +490,16 @@ def schedule_batch(cn, db, stream, args):
                      "schedule": "plain one-launch, one warp per chain, one lane decoding, index order",
                      "lane_split": {"ms_per_step": plain_ms, "value": db.audio_s / (plain_ms / 1e3),
                                     "schedule": "plain one-launch, one warp per chain, 32 lanes, index order"}}
-    res = db.results()
-    cycles = res[:, 3].astype(np.float64)     # decode time per chain (us), the cost model's target
     # learned order (the packet-count order is the fallback)
     order = costmodel.packet_order(db.cap_pkts, db.chans)
     info["order"] = "packets x channels"
     if args.order == "mlp":
+        model, info["cost_model"] = train_cost_model(args, stream)
         feats = costmodel.chain_features(plain_b)
-        model = costmodel.CostModel(seed=1)
-        t0 = time.time()
-        losses = model.fit(feats, np.maximum(cycles, 1.0), steps=1500, lr=3e-3)
         pred = model.predict(feats)
-        y, yh = np.log(np.maximum(cycles, 1.0)), np.log(pred)
-        r2 = 1.0 - np.sum((y - yh) ** 2) / np.sum((y - y.mean()) ** 2)
         order = np.argsort(-pred, kind="stable")
-        info["order"] = "learned (MLP 16-64-64-1)"
-        info["cost_model"] = {"train_s": round(time.time() - t0, 2), "loss_first": float(losses[0]),
-                              "loss_last": float(losses[-1]), "r2_log_cycles": round(float(r2), 4)}
+        info["order"] = "learned (MLP 16-64-64-1, trained on %s)" % info["cost_model"]["train_corpus"]
+        info["_pred"] = pred
     # autotune width x block on the scheduled form, then the decoder warps per SM
     width, block = args.width, args.block
     sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
@@ -324,85 +522,100 @@ def schedule_batch(cn, db, stream, args):
         light, tails = cn.autotune_tail(b, light=(0, 8, 16, 32), reps=2, stream=stream.cuda_stream)
         info["autotune_light_sms"] = {str(k): round(v, 1) for k, v in tails.items()}
     info.update(width=width, block=block, max_groups=max_groups, light_sms=b.light_sms)
+    if sched == 1:
+        info["orders"] = compare_orders(cn, db, stream, b, info)
+    info.pop("_pred", None)
     return b, info
 
 
 # ------------------------------------------------------------------ serving workload
 
 def serve_bench(args, files, dev):
-    """Poisson arrivals through the continuous-batching server, against the
-    plain form that decodes one request per launch in arrival order."""
+    """Poisson arrivals through the continuous-batching server at each rate of
+    --rates, against the plain form that decodes one request per launch in
+    arrival order (the reference daemon's loop), both on the same arrival
+    schedule and files.  Per rate: sustained audio-s/s (all requests' audio /
+    first arrival to last completion) and p50 / p99 latency (arrival to
+    result in host memory)."""
+    import ctypes
     import torch
     from cuopus_b200 import cuopus_native as cn
     from cuopus_b200.serving import Server
-    rng = np.random.default_rng(7)
     n = len(files)
-    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
-    audio = [cn.probe_pcm(f)[0] / 48000.0 for f in files]
+    play = [cn.probe_pcm(f) for f in files]
+    audio = [p / 48000.0 for p, _ in play]
     total_audio = float(sum(audio))
-    out = {}
-    # continuous batching
-    with Server(budget_bytes=args.budget_gb << 30, width=args.width, block=args.block) as srv:
-        srv.wait(srv.submit(files[0]))                      # warm-up (context, slots)
-        ids = [None] * n
-        done_lat = [0.0] * n
-        t0 = time.perf_counter()
-
-        def waiter():
-            for i in range(n):
-                while ids[i] is None:
-                    time.sleep(0.0005)
-                _, _, done_lat[i] = srv.wait(ids[i])
-
-        th = threading.Thread(target=waiter)
-        th.start()
-        for i in range(n):
-            d = arrivals[i] - (time.perf_counter() - t0)
-            if d > 0:
-                time.sleep(d)
-            ids[i] = srv.submit(files[i])
-        th.join()
-        wall = time.perf_counter() - t0
-        st = srv.stats()
-        lat = np.array(done_lat)
-        out["served"] = {"value": total_audio / wall, "p50_ms": float(np.percentile(lat, 50)),
-                         "p99_ms": float(np.percentile(lat, 99)), "wall_s": wall, "waves": st["waves"],
-                         "wave_chains": st["wave_chains"], "requests": n}
-    # one launch per request, arrival order, one at a time
+    rates = [float(r) for r in args.rates.split(",")]
+    out = {"requests": n, "audio_s": total_audio, "longest_request_s": max(audio), "rates": {}}
     stream = torch.cuda.current_stream()
-    caps = []
-    for f in files:
-        play, ch = cn.probe_pcm(f)
-        caps.append(play * ch)
+    caps = [p * c for p, c in play]
     buf = torch.empty(max(caps), dtype=torch.int16, device=dev)
     host = torch.empty(max(caps), dtype=torch.int16, pin_memory=True)
-    import ctypes
     lib = cn.lib()
     err = ctypes.create_string_buffer(512)
-    lat = []
-    t0 = time.perf_counter()
-    for i, f in enumerate(files):
-        d = arrivals[i] - (time.perf_counter() - t0)
-        if d > 0:
-            time.sleep(d)
-        ba = (ctypes.c_char_p * 1)(f)
-        la = (ctypes.c_size_t * 1)(len(f))
-        oa = (ctypes.c_void_p * 1)(buf.data_ptr())
-        ca = (ctypes.c_size_t * 1)(caps[i])
-        ol = (ctypes.c_int64 * 1)()
-        oc = (ctypes.c_int32 * 1)()
-        rc = lib.cuopus_decode_i16_multi(ba, la, 1, oa, ca, ol, oc, ctypes.c_void_p(stream.cuda_stream), err, 512)
-        if rc:
-            raise RuntimeError(err.value.decode())
-        host[:caps[i]].copy_(buf[:caps[i]], non_blocking=True)
-        torch.cuda.synchronize()
-        lat.append((time.perf_counter() - t0 - arrivals[i]) * 1e3)
-    wall = time.perf_counter() - t0
-    lat = np.array(lat)
-    out["one_launch_per_request"] = {"value": total_audio / wall, "p50_ms": float(np.percentile(lat, 50)),
-                                     "p99_ms": float(np.percentile(lat, 99)), "wall_s": wall}
-    out["audio_s"] = total_audio
-    out["arrival_rate_per_s"] = args.rate
+    with Server(budget_bytes=args.budget_gb << 30, width=args.serve_width, block=args.block,
+                max_inflight=args.serve_inflight) as srv:
+        srv.wait(srv.submit(files[0]))                      # warm-up (context, slots)
+        for ri, rate in enumerate(rates):
+            rng = np.random.default_rng(7 + ri)
+            arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+            # continuous batching
+            ids = [None] * n
+            done_at = [0.0] * n
+            t0 = time.perf_counter()
+
+            def waiter():
+                for i in range(n):
+                    while ids[i] is None:
+                        time.sleep(0.0002)
+                    srv.wait(ids[i])
+                    done_at[i] = time.perf_counter() - t0
+
+            th = threading.Thread(target=waiter)
+            th.start()
+            for i in range(n):
+                d = arrivals[i] - (time.perf_counter() - t0)
+                if d > 0:
+                    time.sleep(d)
+                ids[i] = srv.submit(files[i])
+            th.join()
+            lat = (np.array(done_at) - arrivals) * 1e3
+            wall = max(done_at)
+            served = {"value": total_audio / wall, "p50_ms": float(np.percentile(lat, 50)),
+                      "p99_ms": float(np.percentile(lat, 99)), "wall_s": wall}
+            # one launch per request, arrival order, one at a time
+            lat2 = []
+            t0 = time.perf_counter()
+            for i, f in enumerate(files):
+                d = arrivals[i] - (time.perf_counter() - t0)
+                if d > 0:
+                    time.sleep(d)
+                ba = (ctypes.c_char_p * 1)(f)
+                la = (ctypes.c_size_t * 1)(len(f))
+                oa = (ctypes.c_void_p * 1)(buf.data_ptr())
+                ca = (ctypes.c_size_t * 1)(caps[i])
+                ol = (ctypes.c_int64 * 1)()
+                oc = (ctypes.c_int32 * 1)()
+                rc = lib.cuopus_decode_i16_multi(ba, la, 1, oa, ca, ol, oc, ctypes.c_void_p(stream.cuda_stream),
+                                                 err, 512)
+                if rc:
+                    raise RuntimeError(err.value.decode())
+                host[:caps[i]].copy_(buf[:caps[i]], non_blocking=True)
+                torch.cuda.synchronize()
+                lat2.append((time.perf_counter() - t0 - arrivals[i]) * 1e3)
+            wall2 = time.perf_counter() - t0
+            lat2 = np.array(lat2)
+            plain = {"value": total_audio / wall2, "p50_ms": float(np.percentile(lat2, 50)),
+                     "p99_ms": float(np.percentile(lat2, 99)), "wall_s": wall2}
+            out["rates"][str(int(rate))] = {"offered_audio_s_per_s": total_audio / float(arrivals[-1]),
+                                            "served": served, "one_launch_per_request": plain,
+                                            "throughput_ratio": served["value"] / plain["value"]}
+            log("serve %g/s: served %.0f audio-s/s p50 %.0f p99 %.0f ms | one launch per request %.0f audio-s/s "
+                "p50 %.0f p99 %.0f ms" % (rate, served["value"], served["p50_ms"], served["p99_ms"], plain["value"],
+                                          plain["p50_ms"], plain["p99_ms"]))
+        st = srv.stats()
+        out["server"] = {"waves": st["waves"], "wave_chains": st["wave_chains"], "width": args.serve_width,
+                         "max_inflight": args.serve_inflight, "budget_gb": args.budget_gb}
     return out
 
 
@@ -457,7 +670,9 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"],
+                    help="reference: libopus on the host cores (the reference arm); reference-gpu: the "
+                         "reference's own CUDA library against this one on the same GPU (mono files, f16k)")
     ap.add_argument("--workload", default="mixed4096", choices=sorted(WORKLOADS))
     ap.add_argument("--count", type=int, default=None, help="override the stream count (development)")
     ap.add_argument("--width", type=int, default=32, help="lanes per chain when not autotuned")
@@ -467,8 +682,11 @@ def main():
     ap.add_argument("--order", default="mlp", choices=["mlp", "packets"])
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the full-size parity check (development)")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
-    ap.add_argument("--rate", type=float, default=100.0, help="serve: Poisson arrivals per second")
+    ap.add_argument("--rates", default="50,100,250,500", help="serve: Poisson arrival rates per second")
+    ap.add_argument("--serve-width", type=int, default=8, help="serve: lanes per chain of the server")
+    ap.add_argument("--serve-inflight", type=int, default=3, help="serve: decode waves in flight")
     ap.add_argument("--budget-gb", type=int, default=40, help="serve: admission budget")
     ap.add_argument("--phases", action="store_true",
                     help="diagnostics, not a bench line: per-stage decoder cycles from libcuopus_phases.so")
@@ -507,6 +725,20 @@ def main():
     if args.phases:
         return phases_report(args)
 
+    if args.impl == "reference-gpu":
+        if rank != 0:
+            return 0
+        files, seg = load_inputs(args.workload, args.count)
+        with ClockSampler(local) as clk:
+            r = reference_gpu_bench(args, files, seg)
+        line = {"metric": METRIC, "impl": "reference-gpu", "unit": "audio-s/s", "n_gpus": 1, "steps": args.steps,
+                "warmup": args.warmup, "higher_is_better": True, "dtype": "int16 decode, float32 16 kHz output",
+                "data": "synthetic (seeded, vendored libopus encoder)",
+                "config": {"workload": args.workload, "files": "mono files of the workload"},
+                "value": r.get("reference", {}).get("value"), "compare": r, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+        return 0
+
     import torch
     if world > 1:
         import torch.distributed as dist
@@ -520,16 +752,19 @@ def main():
     cn.warmup()
 
     if args.workload == "serve":
-        r = serve_bench(args, files, dev)
+        with ClockSampler(local) as clk:
+            r = serve_bench(args, files, dev)
         if rank == 0:
-            s = r["served"]
+            top = r["rates"][max(r["rates"], key=float)]
+            s = top["served"]
             line = {"metric": METRIC, "value": s["value"], "unit": "audio-s/s", "n_gpus": world, "steps": 1,
                     "warmup": 1, "ms_per_step": s["wall_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
                     "vs_baseline": None, "dtype": "int16", "data": "synthetic (seeded, vendored libopus encoder)",
-                    "config": {"workload": "serve", "requests": s["requests"], "arrivals_per_s": args.rate,
-                               "lengths": "log-normal median 30 s, sigma 1, clipped to [5, 600] s",
+                    "config": {"workload": "serve", "requests": r["requests"], "arrivals_per_s": args.rates,
+                               "lengths": "log-normal median 30 s, sigma 1, clipped to [5 s, 2 h]; longest %.0f s"
+                                          % r["longest_request_s"],
                                "budget_gb": args.budget_gb},
-                    "latency_ms": {"p50": s["p50_ms"], "p99": s["p99_ms"]}, "serve": r}
+                    "latency_ms": {"p50": s["p50_ms"], "p99": s["p99_ms"]}, "serve": r, "clocks": clk.summary()}
             print(json.dumps(line), flush=True)
         return 0
 
@@ -575,6 +810,7 @@ def main():
 
     # e2e through the C ABI from host bytes, PCM read back to pinned host memory
     e2e = None
+    e2e_host = None
     if not args.no_e2e:
         import ctypes
         play = [cn.probe_pcm(f) for f in files]
@@ -592,7 +828,6 @@ def main():
         err = ctypes.create_string_buffer(512)
         os.environ["CUOPUS_SEG_S"] = str(seg)
         os.environ["CUOPUS_MAX_BATCH"] = str(10 ** 8)
-        os.environ["CUOPUS_STRIDE"] = str(info["width"])
         os.environ["CUOPUS_DEMUX_THREADS"] = str(threads)     # demux the files on every host core
 
         f16k = args.workload == "long7200"
@@ -637,12 +872,19 @@ def main():
             t = torch.tensor([e2e_s], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_s = float(t.item())
+        e2e_host = ("f16k", host16, n16) if f16k else ("i16", host, caps)
         e2e = {"value": world * db.audio_s / e2e_s, "unit": "audio-s/s",
                "h2d_bytes_per_step": int(sum(map(len, files))),
                "d2h_bytes_per_step": int(4 * sum(n16)) if f16k else int(2 * sum(caps)),
                "ms_per_step": e2e_s * 1e3, "api": "cuopus_decode_f16k_multi (float32 16 kHz)" if f16k else
                "cuopus_decode_i16_multi (int16 48 kHz)", "demux_threads": threads,
                "last_call": {k: (round(v, 2) if isinstance(v, float) else v) for k, v in cn.last_stats().items()}}
+
+    # full-size parity (after every timed region, untimed): every chain of the
+    # timed batch against libopus, and the e2e output against the batch
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = full_parity(db, threads, e2e_host)
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_budget > 0:
@@ -668,7 +910,7 @@ def main():
                              "alg_bytes_per_launch": alg_bytes, "kernel_ms": kern_ms,
                              "kernel": "k_decode_chains"},
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "gpu_launches": args.steps,
-                "decode_errors": bad, "tail": tail}
+                "decode_errors": bad, "tail": tail, "parity": parity}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -65,6 +65,20 @@ def packet_order(npkts, channels):
     return np.argsort(-cost, kind="stable")
 
 
+def makespan(cost, order, slots):
+    """The scheduler's estimate of a batch's decode time: chains taken in
+    `order` by the first of `slots` decoder groups to come free, each busy for
+    its chain's cost (list scheduling, as the device queue hands them out)."""
+    import heapq
+    free = [0.0] * max(int(slots), 1)
+    end = 0.0
+    for c in order:
+        t = heapq.heappop(free) + float(cost[c])
+        end = max(end, t)
+        heapq.heappush(free, t)
+    return end
+
+
 class CostModel:
     """FP32 MLP over chain features; targets are standardised log decode times."""
 

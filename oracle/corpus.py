@@ -357,8 +357,8 @@ def workload_specs(name, seed=1234, count=None, seconds=None):
                               channels=int(rng.choice([1, 2]))))
     elif name == "lognormal":
         # serving requests: log-normal lengths, median 30 s, sigma 1, clipped
-        # to [5 s, seconds] (the upper clip stands in for 2 h files, whose
-        # encoding alone would take minutes per file)
+        # to [5 s, seconds] (2 h for the serving workload; a draw that long is
+        # rare, and encoding it takes minutes)
         for i in range(count or 256):
             L = float(np.clip(30.0 * math.exp(rng.normal(0.0, 1.0)), 5.0, seconds or 600.0))
             specs.append(dict(kind="mixed", seed=seed * 1000003 + i, seconds=round(L, 3),
