@@ -468,7 +468,9 @@ extern "C" int cuopus_server_create(const cuopus_server_config *cfg, cuopus_serv
     if (s->cfg.seg_s <= 0) s->cfg.seg_s = 1.0;
     if (s->cfg.preroll_ms < 0) s->cfg.preroll_ms = 250.0;
     if (s->cfg.preroll_ms == 0 && !(cfg && cfg->preroll_ms == 0)) s->cfg.preroll_ms = 250.0;
-    s->width = s->cfg.width > 0 ? s->cfg.width : 32;
+    // chains of a few seconds at most: many short chains decode faster at 8
+    // lanes on every resident group than at 32 (the file entry points' rule)
+    s->width = s->cfg.width > 0 ? s->cfg.width : (s->cfg.seg_s <= 4.0 ? 8 : 32);
     s->block = s->cfg.block > 0 ? s->cfg.block : 128;
     if ((s->width & (s->width - 1)) || s->width > 32 || s->block % s->width || s->block > 128 || s->block % 32)
         return fail(errbuf, errcap, 3, "bad width %d / block %d", s->width, s->block);
