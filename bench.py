@@ -675,6 +675,8 @@ def main():
                          "reference's own CUDA library against this one on the same GPU (mono files, f16k)")
     ap.add_argument("--workload", default="mixed4096", choices=sorted(WORKLOADS))
     ap.add_argument("--count", type=int, default=None, help="override the stream count (development)")
+    ap.add_argument("--seg", type=float, default=None,
+                    help="override the chain length in seconds (1e9: whole streams); small profiling cases")
     ap.add_argument("--width", type=int, default=32, help="lanes per chain when not autotuned")
     ap.add_argument("--block", type=int, default=128, help="threads per block when not autotuned")
     ap.add_argument("--warps-per-sm", type=int, default=0, help="decoder warps per SM when not autotuned (0 = all)")
@@ -749,6 +751,8 @@ def main():
     from cuopus_b200 import cuopus_native as cn
 
     files, seg = load_inputs(args.workload, args.count)
+    if args.seg:
+        seg = args.seg
     cn.warmup()
 
     if args.workload == "serve":
