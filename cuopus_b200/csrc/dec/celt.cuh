@@ -952,6 +952,7 @@ DNI void exp_rotation_dec(int16_t *X, int len, int stride, int K, int spread)
 // value; every element is scaled on its own)
 DNI void renormalise_vector(Lanes L, int16_t *X, int N, int16_t gain)
 {
+    PHASE_BEGIN(t_rn);
     int32_t E = 0;
     LFOR(L, i, 0, N) E = c_mac16(E, X[i], X[i]);
     E = wadd(lsum(L, E), 1);
@@ -960,20 +961,25 @@ DNI void renormalise_vector(Lanes L, int16_t *X, int N, int16_t gain)
     int16_t g = (int16_t)c_mul16_p15(c_rsqrt_norm(t), gain);
     LFOR(L, i, 0, N) X[i] = (int16_t)c_pshr(c_mul16(g, X[i]), k + 1);
     lsync(L);
+    PHASE_END(PH_PVQ_RENORM, t_rn, L.id);
 }
 
 // celt/vq.c alg_unquant
 DNI unsigned alg_unquant(Lanes L, int16_t *X, int N, int K, int spread, int B, RangeDec *dec, int16_t gain,
                          int32_t *iy)
 {
+    PHASE_BEGIN(t_cw);
     int32_t Ryy = cwrsi(N, K, rd_uint(dec, pvq_v(N, K)), iy);
+    PHASE_END(PH_PVQ_CWRSI, t_cw, L.id);
     // normalise_residual (every element on its own)
     int k = c_ilog2(Ryy) >> 1;
     int32_t t = c_vshr(Ryy, 2 * (k - 7));
     int16_t g = (int16_t)c_mul16_p15(c_rsqrt_norm(t), gain);
     LFOR(L, i, 0, N) X[i] = (int16_t)c_pshr(c_mul16(g, iy[i]), k + 1);
     lsync(L);
+    PHASE_BEGIN(t_rt);
     exp_rotation_dec(X, N, B, K, spread);
+    PHASE_END(PH_PVQ_ROT, t_rt, L.id);
     // extract_collapse_mask
     if (B <= 1) return 1;
     int N0 = (int)((unsigned)N / (unsigned)B);
@@ -1245,7 +1251,9 @@ DNI unsigned quant_partition(BandCtx *ctx, int16_t *X, int N, int b, int B, int1
                 int B2 = (f->B + 1) >> 1;
                 int LM2 = f->LM - 1;
                 int b2 = f->b;
+                PHASE_BEGIN(t_th);
                 compute_theta(ctx, &sctx, N2, &b2, B2, B0, LM2, 0, &fill2);
+                PHASE_END(PH_PVQ_THETA, t_th, ctx->L.id);
                 int delta = sctx.delta, itheta = sctx.itheta;
                 if (B0 > 1 && (itheta & 0x3fff)) {
                     if (itheta > 8192) delta -= delta >> (4 - LM2);
@@ -1346,6 +1354,7 @@ DNI unsigned quant_band(BandCtx *ctx, int16_t *X, int N, int b, int B, int16_t *
     N_B = (int)((unsigned)N_B / (unsigned)B);
     if (N == 1) return quant_band_n1(ctx, X, 0, lowband_out);
     if (tf_change > 0) recombine = tf_change;
+    PHASE_BEGIN(t_tf);
     if (lowband_scratch && lowband && (recombine || ((N_B & 1) == 0 && tf_change < 0) || B0 > 1)) {
         for (int j = 0; j < N; j++) lowband_scratch[j] = lowband[j];
         lowband = lowband_scratch;
@@ -1368,7 +1377,9 @@ DNI unsigned quant_band(BandCtx *ctx, int16_t *X, int N, int b, int B, int16_t *
     N_B0 = N_B;
     if (B0 > 1 && lowband)
         deinterleave_hadamard(lowband, N_B >> recombine, B0 << recombine, longBlocks, ctx->w->tmp);
+    PHASE_END(PH_PVQ_TF, t_tf, ctx->L.id);
     cm = quant_partition(ctx, X, N, b, B, lowband, LM, gain, fill);
+    PHASE_BEGIN(t_tf2);
     if (B0 > 1) interleave_hadamard(X, N_B >> recombine, B0 << recombine, longBlocks, ctx->w->tmp);
     N_B = N_B0;
     B = B0;
@@ -1382,6 +1393,7 @@ DNI unsigned quant_band(BandCtx *ctx, int16_t *X, int N, int b, int B, int16_t *
         cm = bit_deinterleave_table[cm];
         haar1(X, N0 >> k, 1 << k);
     }
+    PHASE_END(PH_PVQ_TF, t_tf2, ctx->L.id);
     B <<= recombine;
     if (lowband_out) {
         int16_t n = (int16_t)c_sqrt(shl32(N0, 22));
@@ -1434,7 +1446,9 @@ DNI unsigned quant_band_stereo(BandCtx *ctx, int16_t *X, int16_t *Y, int N, int 
     SplitCtx sctx;
     if (N == 1) return quant_band_n1(ctx, X, Y, lowband_out);
     int orig_fill = fill;
+    PHASE_BEGIN(t_th);
     compute_theta(ctx, &sctx, N, &b, B, B, LM, 1, &fill);
+    PHASE_END(PH_PVQ_THETA, t_th, ctx->L.id);
     int inv = sctx.inv, delta = sctx.delta, itheta = sctx.itheta, qalloc = sctx.qalloc;
     int16_t mid = (int16_t)sctx.imid, side = (int16_t)sctx.iside;
     int mbits, sbits;

@@ -141,7 +141,10 @@ DFN int32_t lbcast(const Lanes &L, int32_t v)
 enum {
     PH_PACKET = 0, PH_SILK_INDICES, PH_SILK_PULSES, PH_SILK_PARAMS, PH_SILK_CORE, PH_SILK_PLC, PH_SILK_CNG,
     PH_SILK_STEREO, PH_SILK_RESAMPLE, PH_CELT_COARSE, PH_CELT_ALLOC, PH_CELT_SHIFT, PH_CELT_BANDS,
-    PH_CELT_SYNTH, PH_CELT_COMB, PH_CELT_DEEMPH, PH_KEEP_COPY, PH_COUNT
+    PH_CELT_SYNTH, PH_CELT_COMB, PH_CELT_DEEMPH, PH_KEEP_COPY,
+    // parts of the stages above (nested in them)
+    PH_PVQ_CWRSI, PH_PVQ_ROT, PH_PVQ_RENORM, PH_PVQ_THETA, PH_PVQ_TF, PH_SILK_LPC, PH_SILK_LTP, PH_SILK_SHELL,
+    PH_COUNT
 };
 #if defined(CUO_PHASE_TIMERS) && defined(__CUDA_ARCH__)
 __device__ void cuo_phase_add(int stage, long long cycles);

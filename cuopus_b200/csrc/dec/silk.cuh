@@ -734,7 +734,11 @@ DNI void silk_decode_pulses(RangeDec *rd, int16_t *pulses, int signalType, int q
         }
     }
     for (int i = 0; i < iter; i++) {
-        if (sum_pulses[i] > 0) silk_shell_decoder(&pulses[i * 16], rd, sum_pulses[i], sw->shell);
+        if (sum_pulses[i] > 0) {
+            PHASE_BEGIN(t_sh);
+            silk_shell_decoder(&pulses[i * 16], rd, sum_pulses[i], sw->shell);
+            PHASE_END(PH_SILK_SHELL, t_sh, 0);
+        }
         else for (int k = 0; k < 16; k++) pulses[i * 16 + k] = 0;
     }
     for (int i = 0; i < iter; i++) {
@@ -964,6 +968,7 @@ DNI void silk_decode_core(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *xq, con
             }
         }
         int32_t *res = w->res_Q14;
+        PHASE_BEGIN(t_ltp);
         if (signalType == SIG_VOICED) {
             // the 5-tap LTP reads samples at least lag - 2 back, so blocks of
             // lag - 2 outputs depend only on earlier blocks: lanes split a
@@ -990,6 +995,8 @@ DNI void silk_decode_core(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *xq, con
         } else {
             pres = pexc;
         }
+        PHASE_END(PH_SILK_LTP, t_ltp, L.id);
+        PHASE_BEGIN(t_lpc);
         // LPC synthesis: order-10/16 recursion per sample.  The prediction is
         // order/2 plus one truncated product per tap, summed with wrap-around
         // adds, so the sum may be taken in any order: the taps on samples
@@ -1018,6 +1025,7 @@ DNI void silk_decode_core(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *xq, con
         }
         pexc += c->subfr_length;
         pxq += c->subfr_length;
+        PHASE_END(PH_SILK_LPC, t_lpc, L.id);
         lsync(L);   // the next subframe's LTP rewrites res_Q14, which this one's synthesis reads
     }
     lsync(L);

@@ -396,7 +396,10 @@ def release_workspaces():
 # decode and contains the others; "keep_copy" (the PCM write) runs inside it.
 PHASE_NAMES = ("packet", "silk_indices", "silk_pulses", "silk_params", "silk_core", "silk_plc", "silk_cng",
                "silk_stereo", "silk_resample", "celt_coarse", "celt_alloc", "celt_shift", "celt_bands",
-               "celt_synth", "celt_comb", "celt_deemph", "keep_copy")
+               "celt_synth", "celt_comb", "celt_deemph", "keep_copy",
+               # parts of the stages above
+               "pvq_cwrsi", "pvq_rotation", "pvq_renormalise", "pvq_theta", "pvq_tf_haar_hadamard", "silk_lpc",
+               "silk_ltp", "silk_shell")
 
 
 def phases_lib_path():
