@@ -908,21 +908,39 @@ DNI int32_t cwrsi(int n, int k, uint32_t idx, int32_t *y)
     return yy;
 }
 
-// celt/vq.c exp_rotation1
+// celt/vq.c exp_rotation1.  Each pass rotates the pairs (X[i], X[i + stride])
+// in order, and pair i + stride reads the element pair i has just written:
+// the pass is `stride` independent recurrences, one per residue class of i
+// mod stride.  Here each class runs on its own with the element it carries
+// into the next pair kept in a register rather than stored and loaded back
+// (a store-then-load round trip per step); every element gets the same
+// arithmetic as in the serial pass.
 DNI void exp_rotation1(int16_t *X, int len, int stride, int16_t c, int16_t s)
 {
-    int16_t ms = (int16_t)-s;
-    int16_t *Xp = X;
-    for (int i = 0; i < len - stride; i++) {
-        int16_t x1 = Xp[0], x2 = Xp[stride];
-        Xp[stride] = (int16_t)c_pshr(c_mac16(c_mul16(c, x2), s, x1), 15);
-        *Xp++ = (int16_t)c_pshr(c_mac16(c_mul16(c, x1), ms, x2), 15);
+    const int16_t ms = (int16_t)-s;
+    // forward: i = 0 .. len - stride - 1
+    for (int j = 0; j < stride && j < len - stride; j++) {
+        int16_t x1 = X[j];
+        int i = j;
+        for (; i < len - stride; i += stride) {
+            int16_t x2 = X[i + stride];
+            X[i] = (int16_t)c_pshr(c_mac16(c_mul16(c, x1), ms, x2), 15);
+            x1 = (int16_t)c_pshr(c_mac16(c_mul16(c, x2), s, x1), 15);   // the new X[i + stride]
+        }
+        X[i] = x1;
     }
-    Xp = &X[len - 2 * stride - 1];
-    for (int i = len - 2 * stride - 1; i >= 0; i--) {
-        int16_t x1 = Xp[0], x2 = Xp[stride];
-        Xp[stride] = (int16_t)c_pshr(c_mac16(c_mul16(c, x2), s, x1), 15);
-        *Xp-- = (int16_t)c_pshr(c_mac16(c_mul16(c, x1), ms, x2), 15);
+    // backward: i = len - 2 stride - 1 .. 0; pair i - stride reads the X[i]
+    // pair i has written
+    const int top = len - 2 * stride - 1;
+    for (int j = 0; j < stride && top - j >= 0; j++) {
+        int i = top - j;
+        int16_t x2 = X[i + stride];
+        for (; i >= 0; i -= stride) {
+            int16_t x1 = X[i];
+            X[i + stride] = (int16_t)c_pshr(c_mac16(c_mul16(c, x2), s, x1), 15);
+            x2 = (int16_t)c_pshr(c_mac16(c_mul16(c, x1), ms, x2), 15);   // the new X[i]
+        }
+        X[i + stride] = x2;
     }
 }
 
