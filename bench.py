@@ -553,7 +553,7 @@ def serve_bench(args, files, dev):
     host = torch.empty(max(caps), dtype=torch.int16, pin_memory=True)
     lib = cn.lib()
     err = ctypes.create_string_buffer(512)
-    with Server(budget_bytes=args.budget_gb << 30, width=args.serve_width, block=args.block,
+    with Server(budget_bytes=args.budget_gb << 30, width=args.serve_width, block=64,
                 max_inflight=args.serve_inflight) as srv:
         srv.wait(srv.submit(files[0]))                      # warm-up (context, slots)
         for ri, rate in enumerate(rates):
@@ -688,7 +688,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--rates", default="50,100,250,500", help="serve: Poisson arrival rates per second")
     ap.add_argument("--serve-width", type=int, default=8, help="serve: lanes per chain of the server")
-    ap.add_argument("--serve-inflight", type=int, default=3, help="serve: decode waves in flight")
+    ap.add_argument("--serve-inflight", type=int, default=8, help="serve: decode waves in flight")
     ap.add_argument("--budget-gb", type=int, default=40, help="serve: admission budget")
     ap.add_argument("--phases", action="store_true",
                     help="diagnostics, not a bench line: per-stage decoder cycles from libcuopus_phases.so")

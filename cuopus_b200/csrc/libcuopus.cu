@@ -562,6 +562,11 @@ int plan_files(const uint8_t *const *oggs, const size_t *ns, int nfiles, bool re
     return RC_OK;
 }
 
+// Threads per block of the file entry points' launch: the autotuner's choice at
+// both widths they use (the 2 h file in 1 s chains at 8 lanes: 164 ms at 64
+// threads against 200 ms at 128; whole streams at 32 lanes: equal).
+const int FILE_BLOCK = 64;
+
 // Lanes per chain of a file batch (CUOPUS_STRIDE, when set, decides).  A
 // batch's decode time is about max(longest chain, total work / decoder
 // groups) / per-group speed.  At 32 lanes a group decodes about 3x faster
@@ -580,8 +585,8 @@ int choose_width(const Plan &P)
         mx = std::max(mx, w);
     }
     long long g32 = default_max_groups(32);
-    if (g32 <= 0) g32 = resident_groups(BLOCK, 32);
-    long long g8 = resident_groups(BLOCK, 8);
+    if (g32 <= 0) g32 = resident_groups(FILE_BLOCK, 32);
+    long long g8 = resident_groups(FILE_BLOCK, 8);
     const double speed32 = 3.0;   // per-group speed at 32 lanes relative to 8
     double t32 = std::max(mx, sum / (double)std::max(g32, 1LL)) / speed32;
     double t8 = std::max(mx, sum / (double)std::max(g8, 1LL));
@@ -647,6 +652,7 @@ int run_plan(const Plan &P, cudaStream_t st, Err &err)
     b.nchains = (int32_t)nch;
     if ((rc = ensure_occupancy(err))) return rc;
     b.width = choose_width(P);
+    b.block = FILE_BLOCK;
     b.max_groups = default_max_groups(b.width);
     G.last_width = b.width;
     // longest chains first through the device queue: packets are the proxy

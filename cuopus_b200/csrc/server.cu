@@ -11,7 +11,11 @@
 //     decode waves of at most `wave_chains` chains; up to `max_inflight` waves
 //     run at once, each on its own stream with its own decoder slots and
 //     tables, so a request that arrives while others decode joins the next
-//     wave and its work overlaps theirs on the device;
+//     wave and its work overlaps theirs on the device.  While two or more
+//     waves are in flight a new wave is held back until it can take half of
+//     `wave_chains` or its oldest chain has waited BATCH_WAIT_MS: launching
+//     every trickle of arrivals as its own small wave would spend the in-flight
+//     waves on a few chains each and leave most of the GPU idle;
 //   * completion: after a wave the per-chain results are checked (status and
 //     sample count against the TOC capacity, as in the one-shot entry points);
 //     when every chain of a request is done its PCM is resampled (f16k) and
@@ -111,7 +115,7 @@ struct RangeAlloc {
 
 struct Request {
     uint64_t id = 0;
-    double t_submit = 0, t_done = 0;
+    double t_submit = 0, t_done = 0, t_admit = 0;
     cuo_host::Demux d;
     cuo_host::Chains c;
     std::vector<uint64_t> cap;             // per chain TOC capacity
@@ -175,6 +179,7 @@ struct cuopus_server {
 
     void run();
     bool admit_locked();
+    bool worth_launching_locked();
     bool build_wave_locked(Wave &w);
     void finish_wave(Wave &w);
 };
@@ -235,10 +240,29 @@ bool cuopus_server::admit_locked()
         r->pcm_off = off + blob;
         r->f32_off = off + blob + pcm;
         r->admitted = true;
+        r->t_admit = now_ms();
         active.push_back(r);
         any = true;
     }
     return any;
+}
+
+const double BATCH_WAIT_MS = 5.0;
+
+// Whether a wave should be launched now (see the header comment).
+bool cuopus_server::worth_launching_locked()
+{
+    size_t avail = 0;
+    double oldest = -1;
+    for (Request *r : active) {
+        size_t left = r->c.size() - r->next_chain;
+        if (left && oldest < 0) oldest = r->t_admit;
+        avail += left;
+    }
+    if (!avail) return false;
+    int busy = 0;
+    for (const Wave &w : waves) busy += w.busy;
+    return busy < 2 || stop || avail >= (size_t)std::max(groups / 2, 1) || now_ms() - oldest >= BATCH_WAIT_MS;
 }
 
 // Pack up to wave_chains chains of admitted requests (oldest first) into w.
@@ -270,7 +294,7 @@ void cuopus_server::run()
         bool launched = false;
         for (Wave &w : waves) {
             if (w.busy) continue;
-            if (!build_wave_locked(w)) break;
+            if (!worth_launching_locked() || !build_wave_locked(w)) break;
             // host tables for this wave
             size_t npk = 0, nch = w.chains.size();
             for (auto &pc : w.chains) npk += pc.first->c.npkts[pc.second];
@@ -464,14 +488,14 @@ extern "C" int cuopus_server_create(const cuopus_server_config *cfg, cuopus_serv
     std::unique_ptr<cuopus_server> s(new cuopus_server());
     if (cfg) s->cfg = *cfg;
     if (s->cfg.budget_bytes <= 0) s->cfg.budget_bytes = 40ll << 30;
-    if (s->cfg.max_inflight <= 0) s->cfg.max_inflight = 2;
+    if (s->cfg.max_inflight <= 0) s->cfg.max_inflight = 8;
     if (s->cfg.seg_s <= 0) s->cfg.seg_s = 1.0;
     if (s->cfg.preroll_ms < 0) s->cfg.preroll_ms = 250.0;
     if (s->cfg.preroll_ms == 0 && !(cfg && cfg->preroll_ms == 0)) s->cfg.preroll_ms = 250.0;
     // chains of a few seconds at most: many short chains decode faster at 8
     // lanes on every resident group than at 32 (the file entry points' rule)
     s->width = s->cfg.width > 0 ? s->cfg.width : (s->cfg.seg_s <= 4.0 ? 8 : 32);
-    s->block = s->cfg.block > 0 ? s->cfg.block : 128;
+    s->block = s->cfg.block > 0 ? s->cfg.block : 64;
     if ((s->width & (s->width - 1)) || s->width > 32 || s->block % s->width || s->block > 128 || s->block % 32)
         return fail(errbuf, errcap, 3, "bad width %d / block %d", s->width, s->block);
     cudaError_t e = cudaGetDevice(&s->dev);

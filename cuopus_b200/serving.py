@@ -55,7 +55,7 @@ def _lib():
 
 
 class Server:
-    def __init__(self, budget_bytes=40 << 30, width=0, block=128, max_inflight=3, wave_chains=0, seg_s=1.0,
+    def __init__(self, budget_bytes=40 << 30, width=0, block=0, max_inflight=0, wave_chains=0, seg_s=1.0,
                  preroll_ms=250.0, f16k=False):
         self.f16k = bool(f16k)
         cfg = ServerConfig(int(budget_bytes), int(width), int(block), int(max_inflight), int(wave_chains),

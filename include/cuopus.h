@@ -229,8 +229,10 @@ typedef struct cuopus_server cuopus_server;
 typedef struct cuopus_server_config {
     int64_t budget_bytes;   /* device arena for admitted requests (0 = 40 GiB) */
     int32_t width;          /* lanes per chain (0 = 8 for chains of up to 4 s, else 32) */
-    int32_t block;          /* threads per block (0 = 128) */
-    int32_t max_inflight;   /* decode waves in flight (0 = 2) */
+    int32_t block;          /* threads per block (0 = 64) */
+    int32_t max_inflight;   /* decode waves in flight (0 = 8); with two or more in flight a
+                               wave waits until it is half full or its oldest chain has
+                               waited 5 ms */
     int32_t wave_chains;    /* chains per wave (0 = the resident lane groups of the GPU) */
     double seg_s;           /* chain length (0 = 1 s) */
     double preroll_ms;      /* chain preroll (0 = 250 ms) */
