@@ -437,11 +437,10 @@ struct Plan {
     uint64_t out_elems = 0;
 };
 
-// One file's demux and chain table, with each chain's decode capacity.
+// One file's demux and chain table (with each chain's decode capacity).
 struct FilePlan {
     cuo_host::Demux d;
     cuo_host::Chains c;
-    std::vector<uint64_t> capn;
     std::string e;
     bool ok = false;
 };
@@ -449,16 +448,6 @@ struct FilePlan {
 void plan_one(const uint8_t *ogg, size_t n, double seg_s, double preroll_ms, bool require_mono, FilePlan &F)
 {
     F.ok = cuo_host::demux_and_chain(ogg, n, seg_s, preroll_ms, require_mono, F.d, &F.c, F.e);
-    if (!F.ok) return;
-    F.capn.resize(F.c.size());
-    for (uint32_t i = 0; i < F.c.size(); i++) {
-        uint64_t capn = 0;
-        for (uint32_t k = 0; k < F.c.npkts[i]; k++) {
-            uint32_t p = F.c.first[i] + k;
-            capn += (uint64_t)cuo_host::toc_samples48(F.d.blob.data() + F.d.off[p], F.d.len[p]);
-        }
-        F.capn[i] = capn;
-    }
 }
 
 // Demux every file and merge the tables.  The files are demuxed and merged on
@@ -508,9 +497,9 @@ int plan_files(const uint8_t *const *oggs, const size_t *ns, int nfiles, bool re
         const cuo_host::Chains &c = Fp.c;
         uint64_t fkeep = 0;
         for (uint32_t i = 0; i < c.size(); i++) {
-            if (Fp.capn[i] < (uint64_t)c.trim[i] + c.keep[i])
+            if (c.cap[i] < (uint64_t)c.trim[i] + c.keep[i])
                 return err.set(RC_SOFT, "chain %u capacity %llu < trim %u + keep %u", i,
-                               (unsigned long long)Fp.capn[i], c.trim[i], c.keep[i]);
+                               (unsigned long long)c.cap[i], c.trim[i], c.keep[i]);
             fkeep += c.keep[i];
         }
         pkt0[f + 1] = pkt0[f] + Fp.d.n_packets();
@@ -553,7 +542,7 @@ int plan_files(const uint8_t *const *oggs, const size_t *ns, int nfiles, bool re
                 P.trim[j] = c.trim[i];
                 P.keep[j] = c.keep[i];
                 P.out_off[j] = P.file_out0[f] + fkeep * d.channels;
-                P.cap[j] = Fp.capn[i];
+                P.cap[j] = c.cap[i];
                 fkeep += c.keep[i];
             }
             Fp = FilePlan();   // release this file's tables on this thread

@@ -27,13 +27,6 @@ int toc_samples48(const uint8_t *p, uint32_t len)
 
 namespace {
 
-struct Span {
-    uint64_t start;
-    uint32_t len;
-    uint32_t page;
-    bool done;
-};
-
 int64_t rd_i64le(const uint8_t *p)
 {
     uint64_t v = 0;
@@ -91,8 +84,25 @@ bool demux(const uint8_t *data, size_t n, const Options &opt, Demux &d, std::str
 {
     d = Demux();
     if (!data || n == 0) { err = "empty stream"; return false; }
-    std::vector<Span> spans;
+    // One pass over the pages.  The body bytes of the audio packets (packet 2
+    // on) are appended to the blob a page at a time, then the lacing table
+    // cuts them into packets, each measured once from its TOC.
     std::vector<int64_t> page_granule;
+    std::vector<int64_t> page_end;   // end sample of the last audio packet completed on the page, or -1
+    page_granule.reserve(n / 2048 + 8);
+    page_end.reserve(n / 2048 + 8);
+    d.blob.reserve(n);
+    d.off.reserve(n / 32 + 8);
+    d.len.reserve(n / 32 + 8);
+    d.sample_off.reserve(n / 32 + 8);
+    uint64_t npk = 0;                          // completed packets, headers included
+    uint64_t acc = 0;                          // bytes of the packet in progress
+    uint64_t head_len = 0;                     // length of packet 0
+    uint64_t head_start = 0, head_span = 0;    // first lacing run of packet 0
+    bool head_seen = false, too_large = false;
+    uint64_t w = 0;                            // blob offset of the audio packet in progress
+    int64_t cum = 0, final_page = -1;
+    int last_dur = 0;
     size_t pos = 0;
     static const uint8_t magic[4] = {'O', 'g', 'g', 'S'};
     while (pos < n) {
@@ -118,96 +128,73 @@ bool demux(const uint8_t *data, size_t n, const Options &opt, Demux &d, std::str
         }
         uint32_t pg = (uint32_t)page_granule.size();
         page_granule.push_back(granule);
-        uint64_t run_start = body;
-        uint32_t run_len = 0;
-        int last = 0;
-        for (uint32_t i = 0; i < nseg; i++) {
-            run_len += table[i];
-            last = table[i];
-            if (table[i] < 255) {
-                spans.push_back({run_start, run_len, pg, true});
-                run_start += run_len;
-                run_len = 0;
+        page_end.push_back(-1);
+        // where this page's audio bytes begin (packets 0 and 1 are headers)
+        uint64_t audio_from = UINT64_MAX;
+        if (npk >= 2) {
+            audio_from = body;
+        } else {
+            uint64_t k = npk, q = body, r = 0;
+            for (uint32_t i = 0; i < nseg; i++) {
+                r += table[i];
+                if (table[i] < 255) {
+                    q += r;
+                    r = 0;
+                    if (++k == 2) { audio_from = q; break; }
+                }
             }
         }
-        if (run_len > 0 || (nseg > 0 && last == 255)) spans.push_back({run_start, run_len, pg, false});
+        if (audio_from < body + blen) d.blob.insert(d.blob.end(), data + audio_from, data + body + blen);
+        // lacing runs < 255 end a packet; a trailing run continues on the next page
+        uint64_t run_start = body, run = 0;
+        for (uint32_t i = 0; i < nseg; i++) {
+            run += table[i];
+            if (table[i] == 255) continue;
+            if (!head_seen) { head_seen = true; head_start = run_start; head_span = run; }
+            acc += run;
+            if (acc > 0xFFFFFFFFull) too_large = true;
+            if (npk >= 2 && !too_large) {
+                uint32_t L = (uint32_t)acc;
+                int ns = toc_samples48(d.blob.data() + w, L);
+                d.off.push_back(w);
+                d.len.push_back(L);
+                d.sample_off.push_back(cum);
+                cum += ns;
+                last_dur = ns;
+                page_end[pg] = cum;
+                final_page = pg;
+                w += L;
+            } else if (npk == 0) {
+                head_len = acc;
+            }
+            npk++;
+            acc = 0;
+            run_start += run;
+            run = 0;
+        }
+        if (run > 0) {
+            if (!head_seen) { head_seen = true; head_start = run_start; head_span = run; }
+            acc += run;
+            if (acc > 0xFFFFFFFFull) too_large = true;
+        }
         pos = body + blen;
     }
     if (page_granule.empty()) { err = "no OGG pages found"; return false; }
     d.n_pages = (uint32_t)page_granule.size();
-
-    // reassemble packets
-    std::vector<uint64_t> pkt_span_first;
-    std::vector<uint32_t> pkt_len, pkt_page;
-    {
-        uint64_t acc = 0;
-        size_t first_span = 0;
-        for (size_t i = 0; i < spans.size(); i++) {
-            if (i == 0 || spans[i - 1].done) first_span = i;
-            acc += spans[i].len;
-            if (acc > 0xFFFFFFFFull) { err = "packet too large"; return false; }
-            if (spans[i].done) {
-                pkt_span_first.push_back(first_span);
-                pkt_len.push_back((uint32_t)acc);
-                pkt_page.push_back(spans[i].page);
-                acc = 0;
-            }
-        }
-    }
-    size_t npk = pkt_len.size();
+    if (too_large) { err = "packet too large"; return false; }
     if (npk < 2) { err = "not an OGG Opus stream (fewer than 2 packets)"; return false; }
-    const Span &h = spans[pkt_span_first[0]];
-    // OpusHead fields are read from the first span, as the reference does
-    if (pkt_len[0] < 19 || h.len < 12 || memcmp(data + h.start, "OpusHead", 8) != 0) {
+    // OpusHead fields are read from packet 0's first lacing run, as the reference does
+    if (head_len < 19 || head_span < 12 || memcmp(data + head_start, "OpusHead", 8) != 0) {
         err = "not an OGG Opus stream (no OpusHead)";
         return false;
     }
-    d.channels = data[h.start + 9];
-    d.preskip = data[h.start + 10] | (data[h.start + 11] << 8);
-
-    size_t n_audio = npk - 2;
-    uint64_t audio_bytes = 0;
-    for (size_t i = 2; i < npk; i++) audio_bytes += pkt_len[i];
-    if (audio_bytes > 0xFFFFFFFFull) { err = "stream too large"; return false; }
-    d.blob.resize(audio_bytes);
-    d.off.resize(n_audio);
-    d.len.resize(n_audio);
-    d.sample_off.resize(n_audio);
-    std::vector<uint32_t> apage(n_audio);
-    uint64_t w = 0;
-    for (size_t k = 0; k < n_audio; k++) {
-        size_t pi = k + 2;
-        d.off[k] = w;
-        d.len[k] = pkt_len[pi];
-        apage[k] = pkt_page[pi];
-        // copy the spans of this packet
-        size_t s = pkt_span_first[pi];
-        uint32_t remaining = pkt_len[pi];
-        while (remaining > 0 || !spans[s].done) {
-            memcpy(d.blob.data() + w, data + spans[s].start, spans[s].len);
-            w += spans[s].len;
-            remaining -= spans[s].len;
-            if (spans[s].done) break;
-            s++;
-        }
-    }
-    if (w != audio_bytes) { err = "internal: blob size mismatch"; return false; }
-
-    // TOC offsets and granule cross-check
-    int64_t cum = 0;
-    for (size_t k = 0; k < n_audio; k++) {
-        d.sample_off[k] = cum;
-        cum += toc_samples48(d.blob.data() + d.off[k], d.len[k]);
-    }
+    d.channels = data[head_start + 9];
+    d.preskip = data[head_start + 10] | (data[head_start + 11] << 8);
+    if (w > 0xFFFFFFFFull) { err = "stream too large"; return false; }
+    d.blob.resize(w);   // drops a partial packet at the end of the stream
     d.toc_total = cum;
-    std::vector<int64_t> page_end(page_granule.size(), -1);
-    int64_t final_page = -1;
-    for (size_t k = 0; k < n_audio; k++) {
-        uint32_t pg = apage[k];
-        page_end[pg] = d.sample_off[k] + toc_samples48(d.blob.data() + d.off[k], d.len[k]);
-        if ((int64_t)pg > final_page) final_page = pg;
-    }
-    int last_dur = n_audio ? toc_samples48(d.blob.data() + d.off[n_audio - 1], d.len[n_audio - 1]) : 0;
+
+    // granule cross-check
     int64_t last_granule = 0;
     for (size_t pg = 0; pg < page_granule.size(); pg++) {
         int64_t g = page_granule[pg];
@@ -249,10 +236,17 @@ bool build_chains(const Demux &d, double seconds, double preroll_ms, Chains &c, 
     // packet after them; the reference's cu_build_chains2 then reads past its
     // prefix-sum array.
     if (npk == 0) { err = "no audio packets"; return false; }
-    std::vector<int64_t> cum(npk + 1, 0);
-    for (uint32_t k = 0; k < npk; k++)
-        cum[k + 1] = cum[k] + toc_samples48(d.blob.data() + d.off[k], d.len[k]);
     const std::vector<int64_t> &so = d.sample_off;
+    // TOC samples before packet k (the demuxer's prefix sums)
+    auto cum = [&](int64_t k) -> int64_t { return k < (int64_t)npk ? so[(size_t)k] : d.toc_total; };
+    // a hint only: a damaged granule can claim far more chains than the packets
+    // hold, and such a stream fails below
+    const size_t nchains = std::min<size_t>((size_t)((total + step - 1) / step), (size_t)npk + 16);
+    c.first.reserve(nchains);
+    c.npkts.reserve(nchains);
+    c.trim.reserve(nchains);
+    c.keep.reserve(nchains);
+    c.cap.reserve(nchains);
     int64_t kept = 0;
     for (int64_t k = 0; k * step < total; k++) {
         int64_t ps = k * step, pe = std::min((k + 1) * step, total);
@@ -260,7 +254,7 @@ bool build_chains(const Demux &d, double seconds, double preroll_ms, Chains &c, 
         int64_t target = std::max<int64_t>(0, ts - preroll);
         int64_t first = (int64_t)(std::upper_bound(so.begin(), so.end(), target) - so.begin()) - 1;
         if (first < 0) first = 0;
-        if (cum[first + 1] <= target) first++;
+        if (cum(first + 1) <= target) first++;
         int64_t last = (int64_t)(std::lower_bound(so.begin(), so.end(), te) - so.begin()) - 1;
         if (last < first) last = first;
         if (first >= (int64_t)npk || last >= (int64_t)npk) {
@@ -269,7 +263,7 @@ bool build_chains(const Demux &d, double seconds, double preroll_ms, Chains &c, 
         }
         int64_t trim = ts - so[first], keep = pe - ps;
         if (trim < 0) { err = fmt("chain %lld: negative trim %lld", k, trim); return false; }
-        int64_t capn = cum[last + 1] - cum[first];
+        int64_t capn = cum(last + 1) - cum(first);
         if (capn < trim + keep) {
             err = fmt("chain %lld: capacity %lld < trim %lld + keep %lld", k, capn, trim, keep);
             return false;
@@ -278,6 +272,7 @@ bool build_chains(const Demux &d, double seconds, double preroll_ms, Chains &c, 
         c.npkts.push_back((uint32_t)(last - first + 1));
         c.trim.push_back((uint32_t)trim);
         c.keep.push_back((uint32_t)keep);
+        c.cap.push_back((uint64_t)capn);
         kept += keep;
     }
     if (kept != total) { err = fmt("internal: sum(keep) %lld != playable %lld", kept, total); return false; }

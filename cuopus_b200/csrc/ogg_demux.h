@@ -62,6 +62,7 @@ Options options_from_env();
 
 struct Chains {
     std::vector<uint32_t> first, npkts, trim, keep;
+    std::vector<uint64_t> cap;   // 48 kHz samples per channel the chain's packets decode to
     uint32_t size() const { return (uint32_t)first.size(); }
 };
 

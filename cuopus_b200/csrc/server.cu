@@ -147,8 +147,10 @@ struct Wave {
     void *h_tab = nullptr;
     size_t h_cap = 0;
     void *slots = nullptr;
+    // chain results land in the pinned table (a copy into pageable memory
+    // would return only after the kernel, holding every other wave back)
     uint32_t *d_res = nullptr;
-    std::vector<uint32_t> h_res;
+    const uint32_t *h_res = nullptr;
     std::vector<std::pair<Request *, uint32_t>> chains;   // (request, chain index)
     // resample jobs issued on this stream after the decode
     std::vector<Request *> finishing;
@@ -187,10 +189,12 @@ struct cuopus_server {
 namespace {
 
 struct Tab {   // per-wave table layout inside one device / pinned buffer
-    size_t off, len, first, npkts, chans, trim, keep, out_off, res, total;
+    size_t off, len, first, npkts, chans, trim, keep, out_off, res, blobs, total;
 };
 
-Tab layout(size_t npk, size_t nch)
+// `blob_bytes`: packets of the requests this wave uploads, staged in the
+// pinned buffer only (the device table does not hold them)
+Tab layout(size_t npk, size_t nch, size_t blob_bytes = 0)
 {
     Tab t;
     size_t o = 0;
@@ -204,6 +208,7 @@ Tab layout(size_t npk, size_t nch)
     t.keep = put(8 * nch);
     t.out_off = put(8 * nch);
     t.res = put(16 * nch);
+    t.blobs = put(blob_bytes);
     t.total = o;
     return t;
 }
@@ -296,9 +301,13 @@ void cuopus_server::run()
             if (w.busy) continue;
             if (!worth_launching_locked() || !build_wave_locked(w)) break;
             // host tables for this wave
-            size_t npk = 0, nch = w.chains.size();
-            for (auto &pc : w.chains) npk += pc.first->c.npkts[pc.second];
-            Tab t = layout(npk, nch);
+            size_t npk = 0, nch = w.chains.size(), blob_bytes = 0;
+            for (size_t c = 0; c < nch; c++) {
+                const Request *r = w.chains[c].first;
+                npk += r->c.npkts[w.chains[c].second];
+                if (!r->up_st && (c == 0 || w.chains[c - 1].first != r)) blob_bytes += rup(r->d.blob.size());
+            }
+            Tab t = layout(npk, nch, blob_bytes);
             lk.unlock();
             cudaError_t e = cudaSuccess;
             if (t.total > w.h_cap) {
@@ -307,11 +316,11 @@ void cuopus_server::run()
                 e = cudaMallocHost(&w.h_tab, t.total * 2);
                 w.h_cap = e == cudaSuccess ? t.total * 2 : 0;
             }
-            if (e == cudaSuccess && t.total > w.d_cap) {
+            if (e == cudaSuccess && t.blobs > w.d_cap) {
                 if (w.d_tab) cudaFree(w.d_tab);
                 w.d_tab = nullptr;
-                e = cudaMalloc(&w.d_tab, t.total * 2);
-                w.d_cap = e == cudaSuccess ? t.total * 2 : 0;
+                e = cudaMalloc(&w.d_tab, t.blobs * 2);
+                w.d_cap = e == cudaSuccess ? t.blobs * 2 : 0;
             }
             if (e == cudaSuccess) {
                 uint8_t *h = (uint8_t *)w.h_tab;
@@ -321,14 +330,18 @@ void cuopus_server::run()
                 uint8_t *chans = h + t.chans;
                 uint64_t *trim = (uint64_t *)(h + t.trim), *keep = (uint64_t *)(h + t.keep);
                 uint64_t *out_off = (uint64_t *)(h + t.out_off);
-                size_t p = 0;
+                size_t p = 0, staged = t.blobs;
                 for (size_t c = 0; c < nch; c++) {
                     Request *r = w.chains[c].first;
                     uint32_t i = w.chains[c].second;
                     if (!r->up_st) {
-                        // first wave to hold one of the request's chains: upload its packets
-                        e = cudaMemcpyAsync(arena + r->blob_off, r->d.blob.data(), r->d.blob.size(),
+                        // first wave to hold one of the request's chains: upload its
+                        // packets through the pinned table, so that the copy returns
+                        // at once instead of waiting for the stream's earlier work
+                        memcpy(h + staged, r->d.blob.data(), r->d.blob.size());
+                        e = cudaMemcpyAsync(arena + r->blob_off, h + staged, r->d.blob.size(),
                                             cudaMemcpyHostToDevice, w.st);
+                        staged += rup(r->d.blob.size());
                         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->up_ev, cudaEventDisableTiming);
                         if (e == cudaSuccess) e = cudaEventRecord(r->up_ev, w.st);
                         r->up_st = w.st;
@@ -348,7 +361,7 @@ void cuopus_server::run()
                     out_off[c] = r->pcm_off / 2 + r->chain_out[i];
                 }
                 if (e == cudaSuccess)
-                    e = cudaMemcpyAsync(w.d_tab, w.h_tab, t.total, cudaMemcpyHostToDevice, w.st);
+                    e = cudaMemcpyAsync(w.d_tab, w.h_tab, t.res, cudaMemcpyHostToDevice, w.st);
             }
             if (e == cudaSuccess) {
                 uint8_t *d = (uint8_t *)w.d_tab;
@@ -374,8 +387,9 @@ void cuopus_server::run()
                 w.t_launch = now_ms();
                 e = cuo::decode_kernel_launch(a, blocks, block, w.st);
                 if (e == cudaSuccess) {
-                    w.h_res.resize(4 * nch);
-                    e = cudaMemcpyAsync(w.h_res.data(), w.d_res, 16 * nch, cudaMemcpyDeviceToHost, w.st);
+                    w.h_res = (const uint32_t *)((uint8_t *)w.h_tab + t.res);
+                    e = cudaMemcpyAsync((uint8_t *)w.h_tab + t.res, w.d_res, 16 * nch, cudaMemcpyDeviceToHost,
+                                        w.st);
                 }
                 if (e == cudaSuccess) e = cudaEventRecord(w.ev, w.st);
             }
@@ -543,11 +557,7 @@ extern "C" int cuopus_server_submit(cuopus_server *s, const uint8_t *ogg, size_t
     r->cap.resize(r->c.size());
     r->chain_out.resize(r->c.size());
     for (uint32_t i = 0; i < r->c.size(); i++) {
-        uint64_t cap = 0;
-        for (uint32_t k = 0; k < r->c.npkts[i]; k++) {
-            uint32_t q = r->c.first[i] + k;
-            cap += (uint64_t)cuo_host::toc_samples48(r->d.blob.data() + r->d.off[q], r->d.len[q]);
-        }
+        uint64_t cap = r->c.cap[i];
         if (cap < (uint64_t)r->c.trim[i] + r->c.keep[i])
             return fail(errbuf, errcap, 1, "chain %u capacity %llu < trim + keep", i, (unsigned long long)cap);
         r->cap[i] = cap;
