@@ -626,6 +626,49 @@ def serve_bench(args, files, dev):
     return out
 
 
+def fit_order(args):
+    """Weights of the file entry points' visiting order (csrc/ordercost.cpp):
+    the training corpus (never a timed workload) is cut in 1 s chains with
+    250 ms preroll, as the file entry points cut, and decoded three times at 8
+    and at 32 lanes per chain with the library's launch (64-thread blocks,
+    queue schedule; every decoder group at 8 lanes, 5 warps per SM at 32); the
+    median of each chain's recorded device time is the target of a
+    non-negative least-squares fit on the chain's features.  Writes the
+    weights to args.fit_order and prints one JSON line of fit statistics."""
+    import torch
+    from cuopus_b200 import cuopus_native as cn
+    from cuopus_b200 import ordercost
+    torch.cuda.set_device(0)
+    cn.warmup()
+    name = "mixed1024train"
+    files, _ = load_inputs(name)
+    db = DeviceBatch(files, 1.0, "cuda:0")
+    stream = torch.cuda.current_stream()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    feats = ordercost.features(db.host)
+    samples = db.keep.astype(np.float64) * db.chans
+    order = np.argsort(-samples, kind="stable")
+    out = {"train_corpus": name, "chains": int(db.n), "audio_s": round(db.audio_s, 1)}
+    w = {}
+    for width in (8, 32):
+        b = db.batch(width, 1, order, 64, 0)
+        b.max_groups = 5 * sms if width == 32 else 0
+        runs = []
+        for _ in range(3):
+            cn.decode_batch(b, stream.cuda_stream)
+            torch.cuda.synchronize()
+            runs.append(db.results()[:, 3].astype(np.float64))
+        t = np.median(np.stack(runs), axis=0)
+        w[width], st = ordercost.fit(feats, t)
+        st["mean_chain_us"] = round(float(t.mean()), 1)
+        out["w%d" % width] = st
+    ordercost.write_coefficients(args.fit_order, w[8], w[32], out)
+    out["weights_us"] = {"w%d" % k: dict(zip(ordercost.FEATURE_NAMES, [round(float(x), 3) for x in v]))
+                         for k, v in w.items()}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 # ------------------------------------------------------------------ main
 
 def phases_report(args):
@@ -699,6 +742,9 @@ def main():
     ap.add_argument("--budget-gb", type=int, default=40, help="serve: admission budget")
     ap.add_argument("--phases", action="store_true",
                     help="diagnostics, not a bench line: per-stage decoder cycles from libcuopus_phases.so")
+    ap.add_argument("--fit-order", metavar="INC", default=None,
+                    help="not a bench line: fit the file entry points' visiting-order weights on the training "
+                         "corpus and write them to INC (cuopus_b200/csrc/ordercost_coef.inc)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -733,6 +779,8 @@ def main():
 
     if args.phases:
         return phases_report(args)
+    if args.fit_order:
+        return fit_order(args)
 
     if args.impl == "reference-gpu":
         if rank != 0:
@@ -883,13 +931,24 @@ def main():
             t = torch.tensor([e2e_s], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_s = float(t.item())
+        last = {k: (round(v, 2) if isinstance(v, float) else v) for k, v in cn.last_stats().items()}
+        # the library's visiting order against the order by decoded samples
+        # (one untimed call each way, same inputs)
+        from cuopus_b200 import ordercost
+        orders = {"model": "fitted additive cost" if ordercost.fitted() else "unfitted default (samples)"}
+        for name, env in (("cost", None), ("samples", "samples")):
+            if env:
+                os.environ["CUOPUS_ORDER"] = env
+            e2e_step()
+            os.environ.pop("CUOPUS_ORDER", None)
+            orders[name + "_kernel_ms"] = round(cn.last_stats()["kernel_ms"], 2)
         e2e_host = ("f16k", host16, n16) if f16k else ("i16", host, caps)
         e2e = {"value": world * db.audio_s / e2e_s, "unit": "audio-s/s",
                "h2d_bytes_per_step": int(sum(map(len, files))),
                "d2h_bytes_per_step": int(4 * sum(n16)) if f16k else int(2 * sum(caps)),
                "ms_per_step": e2e_s * 1e3, "api": "cuopus_decode_f16k_multi (float32 16 kHz)" if f16k else
                "cuopus_decode_i16_multi (int16 48 kHz)", "demux_threads": threads,
-               "last_call": {k: (round(v, 2) if isinstance(v, float) else v) for k, v in cn.last_stats().items()}}
+               "last_call": last, "library_order": orders}
 
     # full-size parity (after every timed region, untimed): every chain of the
     # timed batch against libopus, and the e2e output against the batch

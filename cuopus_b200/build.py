@@ -61,7 +61,8 @@ def _run(cmd):
 
 def build_libcuopus(force=False):
     deps = _sources("libcuopus.cu", "decode_kernel.cu", "costmodel.cu", "server.cu", "kernels.cuh", "ogg_demux.cpp",
-                    "ogg_demux.h", "dec") + [os.path.join(ROOT, "include", "cuopus.h")]
+                    "ogg_demux.h", "ordercost.cpp", "ordercost.h", "ordercost_coef.inc", "dec") + \
+        [os.path.join(ROOT, "include", "cuopus.h")]
     if not force and not _stale(LIBCUOPUS, deps):
         return LIBCUOPUS
     os.makedirs(LIB, exist_ok=True)
@@ -78,8 +79,9 @@ def build_libcuopus(force=False):
     _run(common + ["-Xptxas", "-v", "-c", os.path.join(CSRC, "costmodel.cu"), "-o", os.path.join(obj, "costmodel.o")])
     _run(common + ["-c", os.path.join(CSRC, "server.cu"), "-o", os.path.join(obj, "server.o")])
     _run(common + ["-c", os.path.join(CSRC, "ogg_demux.cpp"), "-o", os.path.join(obj, "ogg_demux.o")])
+    _run(common + ["-c", os.path.join(CSRC, "ordercost.cpp"), "-o", os.path.join(obj, "ordercost.o")])
     tmp = LIBCUOPUS + ".tmp"
-    rest = [os.path.join(obj, o) for o in ("libcuopus.o", "costmodel.o", "server.o", "ogg_demux.o")]
+    rest = [os.path.join(obj, o) for o in ("libcuopus.o", "costmodel.o", "server.o", "ogg_demux.o", "ordercost.o")]
     _run([NVCC, *ARCH, "-shared", "-o", tmp, os.path.join(obj, "decode_kernel.o")] + rest)
     os.replace(tmp, LIBCUOPUS)
     # diagnostic build: the same library with the decoder's stage timers on

@@ -34,6 +34,7 @@
 #include "../../include/cuopus.h"
 #include "kernels.cuh"
 #include "ogg_demux.h"
+#include "ordercost.h"
 
 namespace {
 
@@ -644,11 +645,27 @@ int run_plan(const Plan &P, cudaStream_t st, Err &err)
     b.block = FILE_BLOCK;
     b.max_groups = default_max_groups(b.width);
     G.last_width = b.width;
-    // longest chains first through the device queue: packets are the proxy
+    // longest chains first through the device queue, by the fitted additive
+    // cost of their packets (CUOPUS_ORDER=samples: by decoded samples x channels)
     std::vector<uint32_t> order(nch);
     std::iota(order.begin(), order.end(), 0u);
-    std::stable_sort(order.begin(), order.end(),
-                     [&](uint32_t x, uint32_t y) { return P.cap[x] * P.chans[x] > P.cap[y] * P.chans[y]; });
+    const char *oenv = getenv("CUOPUS_ORDER");
+    if (oenv && strcmp(oenv, "samples") == 0) {
+        std::stable_sort(order.begin(), order.end(),
+                         [&](uint32_t x, uint32_t y) { return P.cap[x] * P.chans[x] > P.cap[y] * P.chans[y]; });
+    } else {
+        const cuo_host::OrderCost oc(cuo_host::order_coefficients(b.width));
+        std::vector<double> cost(nch);
+        for (uint32_t c = 0; c < nch; c++) {
+            double s = oc.chain;
+            for (uint32_t k = 0; k < P.npkts[c]; k++) {
+                uint64_t q = (uint64_t)P.first[c] + k;
+                s += oc.of(P.blob.data() + P.off[q], P.len[q], P.chans[c]);
+            }
+            cost[c] = s;
+        }
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return cost[x] > cost[y]; });
+    }
     b.schedule = 1;
     b.order = order.data();
     float kms = 0.f;

@@ -215,6 +215,29 @@ int cuopus_mlp_grad(const float *params_dev, const float *x_dev, const float *t_
 int cuopus_mlp_train(float *params_dev, const float *x_dev, const float *t_dev, int n, int steps, float lr,
                      float *losses, void *cuda_stream, char *errbuf, size_t errcap);
 
+/* ---- Extension: the visiting order of the file entry points (no counterpart
+ * in the reference).  They queue chains longest first by an additive cost: the
+ * sum over a chain's packets of non-negative weights times the packet's
+ * features, plus a constant per chain.  The weights are fitted by
+ * non-negative least squares to per-chain device times of a training corpus,
+ * one set for 8 lanes per chain and one for 32.  Host pointers; the tables are
+ * those of cuopus_batch.  feat receives nchains x CUOPUS_ORDER_FEATURES values:
+ * 1 (chain constant), packets, bytes / 100, frames per (mode, duration) class
+ * and TOC stereo bit (SILK 10/20/40/60 ms, hybrid 10/20, CELT 2.5/5/10/20;
+ * mono then stereo for each), SILK ms x bandwidth (NB 0..WB 2), CELT ms x
+ * bandwidth (NB 0..FB 3), ms decoded to a stereo output, empty packets.
+ * cost[c] = weights(width) . feat[c].  cuopus_order_model_fitted() is 0 while
+ * the weights are the unfitted default (decoded duration x channels). */
+#define CUOPUS_ORDER_FEATURES 27
+int cuopus_order_features(const uint8_t *blob, const uint64_t *off, const uint32_t *len, const uint32_t *first,
+                          const uint32_t *npkts, const uint8_t *channels, int32_t nchains, double *feat);
+int cuopus_order_costs(const uint8_t *blob, const uint64_t *off, const uint32_t *len, const uint32_t *first,
+                       const uint32_t *npkts, const uint8_t *channels, int32_t nchains, int32_t width,
+                       double *cost);
+int cuopus_order_model_fitted(void);
+/* w receives the CUOPUS_ORDER_FEATURES weights used for `width` lanes. */
+int cuopus_order_weights(int32_t width, double *w);
+
 /* ---- Extension: continuous-batching decode server (no counterpart in the
  * reference, whose daemon decodes one request at a time, decode_cli.cu:572-678).
  * Requests are demuxed on the submitting thread and admitted, oldest first,
