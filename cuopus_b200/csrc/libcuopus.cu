@@ -414,21 +414,12 @@ int decode_batch(const cuopus_batch *b, cudaStream_t st, float *kernel_ms, Err &
     return RC_OK;
 }
 
-// One call's worth of files merged into a single chain table.
-// std::allocator that leaves new elements uninitialised (the merged tables
-// are written in full right after they are sized).
-template <class T> struct NoInit : std::allocator<T> {
-    template <class U> struct rebind { using other = NoInit<U>; };
-    NoInit() = default;
-    template <class U> NoInit(const NoInit<U> &) {}
-    template <class U> void construct(U *p) noexcept { ::new ((void *)p) U; }
-    template <class U, class... A> void construct(U *p, A &&...a) { ::new ((void *)p) U(std::forward<A>(a)...); }
-};
-
+// One call's worth of files merged into a single chain table (the packet
+// tables uninitialised when sized: they are written in full right after).
 struct Plan {
-    std::vector<uint8_t, NoInit<uint8_t>> blob;
-    std::vector<uint64_t, NoInit<uint64_t>> off;
-    std::vector<uint32_t, NoInit<uint32_t>> len;
+    cuo_host::Table<uint8_t> blob;
+    cuo_host::Table<uint64_t> off;
+    cuo_host::Table<uint32_t> len;
     std::vector<uint32_t> first, npkts;
     std::vector<uint8_t> chans;
     std::vector<uint64_t> trim, keep, out_off, cap;
@@ -446,15 +437,17 @@ struct FilePlan {
     bool ok = false;
 };
 
-void plan_one(const uint8_t *ogg, size_t n, double seg_s, double preroll_ms, bool require_mono, FilePlan &F)
+void plan_one(const uint8_t *ogg, size_t n, double seg_s, double preroll_ms, bool require_mono, FilePlan &F,
+              int threads)
 {
-    F.ok = cuo_host::demux_and_chain(ogg, n, seg_s, preroll_ms, require_mono, F.d, &F.c, F.e);
+    F.ok = cuo_host::demux_and_chain(ogg, n, seg_s, preroll_ms, require_mono, F.d, &F.c, F.e, threads);
 }
 
 // Demux every file and merge the tables.  The files are demuxed and merged on
 // CUOPUS_DEMUX_THREADS host threads (default 1: the calling thread only, as
-// the reference's library, which starts no threads); errors are reported for
-// the lowest-numbered failing file, whatever the thread count.
+// the reference's library, which starts no threads); with fewer files than
+// threads, each file's demux splits its pages over the threads left.  Errors
+// are reported for the lowest-numbered failing file, whatever the thread count.
 int plan_files(const uint8_t *const *oggs, const size_t *ns, int nfiles, bool require_mono, Plan &P, Err &err)
 {
     double seg_s = env_f("CUOPUS_SEG_S", 1.0);
@@ -462,12 +455,13 @@ int plan_files(const uint8_t *const *oggs, const size_t *ns, int nfiles, bool re
     for (int f = 0; f < nfiles; f++)
         if (!oggs || !ns || !oggs[f] || !ns[f]) return err.set(RC_ARG, "file %d: empty input", f);
     std::vector<FilePlan> F((size_t)std::max(nfiles, 0));
-    int nthreads = std::min(env_i("CUOPUS_DEMUX_THREADS", 1), std::max(nfiles, 1));
-    if (nthreads > 64) nthreads = 64;
+    const int all_threads = std::min(env_i("CUOPUS_DEMUX_THREADS", 1), 64);
+    int nthreads = std::min(all_threads, std::max(nfiles, 1));
+    const int per_file = std::max(1, all_threads / std::max(nfiles, 1));
     std::atomic<int> next(0);
     auto work = [&]() {
         for (int f; (f = next.fetch_add(1)) < nfiles;)
-            plan_one(oggs[f], ns[f], seg_s, preroll_ms, require_mono, F[f]);
+            plan_one(oggs[f], ns[f], seg_s, preroll_ms, require_mono, F[f], per_file);
     };
     auto run = [&](const std::function<void()> &fn) {
         next = 0;
@@ -512,10 +506,18 @@ int plan_files(const uint8_t *const *oggs, const size_t *ns, int nfiles, bool re
         P.file_play48[f] = Fp.d.play48;
         P.out_elems += fkeep * (uint64_t)Fp.d.channels;
     }
-    // merged tables: every file fills its own ranges (on the same threads)
-    P.blob.resize(byte0[nfiles]);
-    P.off.resize(pkt0[nfiles]);
-    P.len.resize(pkt0[nfiles]);
+    // merged tables: every file fills its own ranges (on the same threads); a
+    // single file's packet tables are taken over as they are
+    const bool take = nfiles == 1;
+    if (take) {
+        P.blob.swap(F[0].d.blob);
+        P.off.swap(F[0].d.off);
+        P.len.swap(F[0].d.len);
+    } else {
+        P.blob.resize(byte0[nfiles]);
+        P.off.resize(pkt0[nfiles]);
+        P.len.resize(pkt0[nfiles]);
+    }
     size_t nch = ch0[nfiles];
     P.first.resize(nch);
     P.npkts.resize(nch);
@@ -529,10 +531,12 @@ int plan_files(const uint8_t *const *oggs, const size_t *ns, int nfiles, bool re
             FilePlan &Fp = F[f];
             const cuo_host::Demux &d = Fp.d;
             const cuo_host::Chains &c = Fp.c;
-            if (!d.blob.empty()) memcpy(P.blob.data() + byte0[f], d.blob.data(), d.blob.size());
-            for (uint32_t k = 0; k < d.n_packets(); k++) {
-                P.off[pkt0[f] + k] = d.off[k] + byte0[f];
-                P.len[pkt0[f] + k] = d.len[k];
+            if (!take) {
+                if (!d.blob.empty()) memcpy(P.blob.data() + byte0[f], d.blob.data(), d.blob.size());
+                for (uint32_t k = 0; k < d.n_packets(); k++) {
+                    P.off[pkt0[f] + k] = d.off[k] + byte0[f];
+                    P.len[pkt0[f] + k] = d.len[k];
+                }
             }
             uint64_t fkeep = 0;
             for (uint32_t i = 0; i < c.size(); i++) {

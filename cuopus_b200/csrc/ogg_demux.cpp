@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <thread>
 
 namespace cuo_host {
 
@@ -63,6 +64,51 @@ uint32_t ogg_page_crc(const uint8_t *page, size_t len)
     return crc;
 }
 
+// What the serial walk knows of one page when it reaches it.
+struct PageWalk {
+    int64_t granule;
+    uint64_t body, blen, table;   // body and lacing table offsets in the stream, body length
+    uint64_t npk;                 // packets completed before the page, headers included
+    uint64_t acc;                 // bytes of the packet in progress at the page start
+    uint64_t audio_from;          // stream offset of the page's first audio byte (UINT64_MAX: none)
+    uint64_t blob;                // blob offset of that byte (audio bytes before the page)
+    uint64_t audio, done;         // audio packets completed before / on the page
+    uint32_t nseg;
+};
+
+// Page ranges of about equal body bytes, at most `threads` of them and none
+// below `range_bytes` (small streams stay on the calling thread).
+std::vector<size_t> page_ranges(const std::vector<PageWalk> &pages, int threads, size_t range_bytes)
+{
+    uint64_t total = 0;
+    for (const PageWalk &P : pages) total += P.blen;
+    size_t t = (size_t)std::max(1, threads);
+    t = std::min<size_t>(t, (size_t)(total / std::max<size_t>(range_bytes, 1)) + 1);
+    std::vector<size_t> cut{0};
+    uint64_t acc = 0;
+    for (size_t pg = 0; pg < pages.size(); pg++) {
+        acc += pages[pg].blen;
+        if (cut.size() < t && acc * t >= total * cut.size() && pg + 1 < pages.size()) cut.push_back(pg + 1);
+    }
+    cut.push_back(pages.size());
+    return cut;
+}
+
+// fn(begin, end) for every range of `cut`, the first on the calling thread.
+template <class F> void run_ranges(const std::vector<size_t> &cut, F &&fn)
+{
+    std::vector<std::thread> pool;
+    for (size_t r = 1; r + 1 < cut.size(); r++) {
+        try {
+            pool.emplace_back([&fn, &cut, r] { fn(cut[r], cut[r + 1]); });
+        } catch (...) {
+            fn(cut[r], cut[r + 1]);   // no thread: run it here
+        }
+    }
+    fn(cut[0], cut[1]);
+    for (auto &th : pool) th.join();
+}
+
 } // namespace
 
 Options options_from_env()
@@ -84,25 +130,21 @@ bool demux(const uint8_t *data, size_t n, const Options &opt, Demux &d, std::str
 {
     d = Demux();
     if (!data || n == 0) { err = "empty stream"; return false; }
-    // One pass over the pages.  The body bytes of the audio packets (packet 2
-    // on) are appended to the blob a page at a time, then the lacing table
-    // cuts them into packets, each measured once from its TOC.
-    std::vector<int64_t> page_granule;
-    std::vector<int64_t> page_end;   // end sample of the last audio packet completed on the page, or -1
-    page_granule.reserve(n / 2048 + 8);
-    page_end.reserve(n / 2048 + 8);
-    d.blob.reserve(n);
-    d.off.reserve(n / 32 + 8);
-    d.len.reserve(n / 32 + 8);
-    d.sample_off.reserve(n / 32 + 8);
+    // 1. A serial walk over the page headers and lacing tables decides
+    //    everything structural: where each page's audio bytes go in the blob,
+    //    which packets complete on it, the header checks and every error.
+    // 2. Page ranges, in parallel: copy the audio bytes into the blob.
+    // 3. Page ranges, in parallel: cut packets, read each TOC once.
+    // 4. Prefix sums of the TOC durations and the granule cross-check.
+    std::vector<PageWalk> pages;
+    pages.reserve(n / 2048 + 8);
     uint64_t npk = 0;                          // completed packets, headers included
     uint64_t acc = 0;                          // bytes of the packet in progress
     uint64_t head_len = 0;                     // length of packet 0
     uint64_t head_start = 0, head_span = 0;    // first lacing run of packet 0
     bool head_seen = false, too_large = false;
-    uint64_t w = 0;                            // blob offset of the audio packet in progress
-    int64_t cum = 0, final_page = -1;
-    int last_dur = 0;
+    uint64_t appended = 0;                     // audio body bytes before the page
+    uint64_t n_audio = 0, w = 0;               // completed audio packets and their bytes
     size_t pos = 0;
     static const uint8_t magic[4] = {'O', 'g', 'g', 'S'};
     while (pos < n) {
@@ -122,17 +164,24 @@ bool demux(const uint8_t *data, size_t n, const Options &opt, Demux &d, std::str
             uint32_t stored = (uint32_t)data[idx + 22] | (uint32_t)data[idx + 23] << 8 |
                               (uint32_t)data[idx + 24] << 16 | (uint32_t)data[idx + 25] << 24;
             if (ogg_page_crc(data + idx, (size_t)(body + blen - idx)) != stored) {
-                err = fmt("page %lld: CRC mismatch", (long long)page_granule.size());
+                err = fmt("page %lld: CRC mismatch", (long long)pages.size());
                 return false;
             }
         }
-        uint32_t pg = (uint32_t)page_granule.size();
-        page_granule.push_back(granule);
-        page_end.push_back(-1);
+        PageWalk P;
+        P.granule = granule;
+        P.body = body;
+        P.blen = blen;
+        P.table = idx + 27;
+        P.nseg = nseg;
+        P.npk = npk;
+        P.acc = acc;
+        P.blob = appended;
+        P.audio = n_audio;
         // where this page's audio bytes begin (packets 0 and 1 are headers)
-        uint64_t audio_from = UINT64_MAX;
+        P.audio_from = UINT64_MAX;
         if (npk >= 2) {
-            audio_from = body;
+            P.audio_from = body;
         } else {
             uint64_t k = npk, q = body, r = 0;
             for (uint32_t i = 0; i < nseg; i++) {
@@ -140,11 +189,11 @@ bool demux(const uint8_t *data, size_t n, const Options &opt, Demux &d, std::str
                 if (table[i] < 255) {
                     q += r;
                     r = 0;
-                    if (++k == 2) { audio_from = q; break; }
+                    if (++k == 2) { P.audio_from = q; break; }
                 }
             }
         }
-        if (audio_from < body + blen) d.blob.insert(d.blob.end(), data + audio_from, data + body + blen);
+        if (P.audio_from < body + blen) appended += body + blen - P.audio_from;
         // lacing runs < 255 end a packet; a trailing run continues on the next page
         uint64_t run_start = body, run = 0;
         for (uint32_t i = 0; i < nseg; i++) {
@@ -153,17 +202,9 @@ bool demux(const uint8_t *data, size_t n, const Options &opt, Demux &d, std::str
             if (!head_seen) { head_seen = true; head_start = run_start; head_span = run; }
             acc += run;
             if (acc > 0xFFFFFFFFull) too_large = true;
-            if (npk >= 2 && !too_large) {
-                uint32_t L = (uint32_t)acc;
-                int ns = toc_samples48(d.blob.data() + w, L);
-                d.off.push_back(w);
-                d.len.push_back(L);
-                d.sample_off.push_back(cum);
-                cum += ns;
-                last_dur = ns;
-                page_end[pg] = cum;
-                final_page = pg;
-                w += L;
+            if (npk >= 2) {
+                n_audio++;
+                w += acc;
             } else if (npk == 0) {
                 head_len = acc;
             }
@@ -177,10 +218,12 @@ bool demux(const uint8_t *data, size_t n, const Options &opt, Demux &d, std::str
             acc += run;
             if (acc > 0xFFFFFFFFull) too_large = true;
         }
+        P.done = n_audio - P.audio;
+        pages.push_back(P);
         pos = body + blen;
     }
-    if (page_granule.empty()) { err = "no OGG pages found"; return false; }
-    d.n_pages = (uint32_t)page_granule.size();
+    if (pages.empty()) { err = "no OGG pages found"; return false; }
+    d.n_pages = (uint32_t)pages.size();
     if (too_large) { err = "packet too large"; return false; }
     if (npk < 2) { err = "not an OGG Opus stream (fewer than 2 packets)"; return false; }
     // OpusHead fields are read from packet 0's first lacing run, as the reference does
@@ -191,18 +234,72 @@ bool demux(const uint8_t *data, size_t n, const Options &opt, Demux &d, std::str
     d.channels = data[head_start + 9];
     d.preskip = data[head_start + 10] | (data[head_start + 11] << 8);
     if (w > 0xFFFFFFFFull) { err = "stream too large"; return false; }
+
+    // the page ranges: audio bytes first (a packet's TOC can sit on an earlier
+    // range's page), then packets; sample_off holds each packet's duration
+    // until the prefix sums below
+    d.blob.resize(appended);
+    d.off.resize(n_audio);
+    d.len.resize(n_audio);
+    d.sample_off.resize(n_audio);
+    const std::vector<size_t> cut = page_ranges(pages, opt.threads, opt.range_bytes);
+    run_ranges(cut, [&](size_t a, size_t b) {
+        for (size_t pg = a; pg < b; pg++) {
+            const PageWalk &P = pages[pg];
+            if (P.audio_from < P.body + P.blen)
+                memcpy(d.blob.data() + P.blob, data + P.audio_from, P.body + P.blen - P.audio_from);
+        }
+    });
+    run_ranges(cut, [&](size_t a, size_t b) {
+        for (size_t pg = a; pg < b; pg++) {
+            const PageWalk &P = pages[pg];
+            const uint8_t *table = data + P.table;
+            uint64_t k = P.audio, pk = P.npk, acc = P.acc, run_start = P.body, run = 0;
+            for (uint32_t i = 0; i < P.nseg; i++) {
+                run += table[i];
+                if (table[i] == 255) continue;
+                acc += run;
+                if (pk >= 2) {
+                    // blob offset of the packet's end, less its length
+                    uint64_t off = P.blob + (run_start + run - P.audio_from) - acc;
+                    d.off[k] = off;
+                    d.len[k] = (uint32_t)acc;
+                    d.sample_off[k] = toc_samples48(d.blob.data() + off, (uint32_t)acc);
+                    k++;
+                }
+                pk++;
+                acc = 0;
+                run_start += run;
+                run = 0;
+            }
+        }
+    });
     d.blob.resize(w);   // drops a partial packet at the end of the stream
+    int64_t cum = 0;
+    int last_dur = 0;
+    for (uint64_t k = 0; k < n_audio; k++) {
+        int64_t ns = d.sample_off[k];
+        d.sample_off[k] = cum;
+        cum += ns;
+        last_dur = (int)ns;
+    }
     d.toc_total = cum;
 
-    // granule cross-check
+    // granule cross-check: a page's end is that of the last audio packet completed on it
+    int64_t final_page = -1;
+    for (size_t pg = 0; pg < pages.size(); pg++)
+        if (pages[pg].done) final_page = (int64_t)pg;
     int64_t last_granule = 0;
-    for (size_t pg = 0; pg < page_granule.size(); pg++) {
-        int64_t g = page_granule[pg];
+    for (size_t pg = 0; pg < pages.size(); pg++) {
+        const PageWalk &P = pages[pg];
+        int64_t g = P.granule;
         if (g != -1 && g > last_granule) last_granule = g;
-        if (g == -1 || page_end[pg] < 0) continue;
+        if (g == -1 || !P.done) continue;
+        uint64_t k_end = P.audio + P.done;
+        int64_t page_end = k_end < n_audio ? d.sample_off[k_end] : d.toc_total;
         d.granule_checked++;
-        if (g == page_end[pg]) d.granule_match++;
-        else if ((int64_t)pg == final_page && page_end[pg] - g >= 0 && page_end[pg] - g < last_dur)
+        if (g == page_end) d.granule_match++;
+        else if ((int64_t)pg == final_page && page_end - g >= 0 && page_end - g < last_dur)
             d.granule_match++;
     }
     d.last_granule = last_granule;
@@ -236,7 +333,7 @@ bool build_chains(const Demux &d, double seconds, double preroll_ms, Chains &c, 
     // packet after them; the reference's cu_build_chains2 then reads past its
     // prefix-sum array.
     if (npk == 0) { err = "no audio packets"; return false; }
-    const std::vector<int64_t> &so = d.sample_off;
+    const Table<int64_t> &so = d.sample_off;
     // TOC samples before packet k (the demuxer's prefix sums)
     auto cum = [&](int64_t k) -> int64_t { return k < (int64_t)npk ? so[(size_t)k] : d.toc_total; };
     // a hint only: a damaged granule can claim far more chains than the packets
@@ -280,9 +377,11 @@ bool build_chains(const Demux &d, double seconds, double preroll_ms, Chains &c, 
 }
 
 bool demux_and_chain(const uint8_t *data, size_t n, double seconds, double preroll_ms, bool require_mono,
-                     Demux &d, Chains *c, std::string &err)
+                     Demux &d, Chains *c, std::string &err, int threads)
 {
-    if (!demux(data, n, d, err)) return false;
+    Options opt = options_from_env();
+    opt.threads = threads;
+    if (!demux(data, n, opt, d, err)) return false;
     if (require_mono && d.channels != 1) {
         err = fmt("only mono supported (channels=%lld)", d.channels);
         return false;

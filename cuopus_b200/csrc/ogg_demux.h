@@ -19,18 +19,32 @@
 // returned as a message, never by exiting.
 #pragma once
 #include <stdint.h>
+
+#include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace cuo_host {
 
 int toc_samples48(const uint8_t *p, uint32_t len);
 
+// std::allocator that leaves new elements uninitialised: tables that are
+// written in full right after they are sized skip the zero fill.
+template <class T> struct NoInit : std::allocator<T> {
+    template <class U> struct rebind { using other = NoInit<U>; };
+    NoInit() = default;
+    template <class U> NoInit(const NoInit<U> &) {}
+    template <class U> void construct(U *p) noexcept { ::new ((void *)p) U; }
+    template <class U, class... A> void construct(U *p, A &&...a) { ::new ((void *)p) U(std::forward<A>(a)...); }
+};
+template <class T> using Table = std::vector<T, NoInit<T>>;
+
 struct Demux {
-    std::vector<uint8_t> blob;        // audio packets back to back
-    std::vector<uint64_t> off;        // per packet offset into blob
-    std::vector<uint32_t> len;        // per packet length
-    std::vector<int64_t> sample_off;  // per packet cumulative 48 kHz offset
+    Table<uint8_t> blob;              // audio packets back to back
+    Table<uint64_t> off;              // per packet offset into blob
+    Table<uint32_t> len;              // per packet length
+    Table<int64_t> sample_off;        // per packet cumulative 48 kHz offset
     int channels = 0;
     int preskip = 0;
     int64_t toc_total = 0;
@@ -54,9 +68,16 @@ struct Demux {
 //                 cuopus_demux.h:240-258)
 // options_from_env() reads them per call from CUOPUS_OGG_CRC=1 and
 // CUOPUS_GRANULE=warn.
+//   threads       host threads that copy the packets and read their TOCs,
+//                 each over a range of pages of about equal bytes (the
+//                 structural walk and every error stay on the calling thread;
+//                 the result does not depend on the count)
+//   range_bytes   the least page bytes per range (small streams: one range)
 struct Options {
     bool check_crc = false;
     bool granule_warn = false;
+    int threads = 1;
+    size_t range_bytes = 256 << 10;
 };
 Options options_from_env();
 
@@ -72,9 +93,10 @@ bool demux(const uint8_t *data, size_t n, Demux &d, std::string &err);
 bool demux(const uint8_t *data, size_t n, const Options &opt, Demux &d, std::string &err);
 bool build_chains(const Demux &d, double seconds, double preroll_ms, Chains &c, std::string &err);
 
-// Demux + the reference's acceptance checks (granule cross-check; mono only
-// when require_mono) + chain table.
+// Demux (options from the environment, `threads` demux threads) + the
+// reference's acceptance checks (granule cross-check; mono only when
+// require_mono) + chain table.
 bool demux_and_chain(const uint8_t *data, size_t n, double seconds, double preroll_ms, bool require_mono,
-                     Demux &d, Chains *c, std::string &err);
+                     Demux &d, Chains *c, std::string &err, int threads = 1);
 
 } // namespace cuo_host

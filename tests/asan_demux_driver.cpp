@@ -5,6 +5,9 @@
 // its end is reported) and parsed with the default options, the page-CRC
 // check and the granule warn-and-resync policy.  One line per record and
 // policy: "ok <play48> <channels> <packets> <chains> <sum keep>" or "refused".
+// Each is also demuxed with its pages split over three threads (ranges of any
+// size); a result that differs in any field is reported on stderr and the
+// driver exits 3.
 #include <stdint.h>
 #include <stdio.h>
 #include <string.h>
@@ -28,7 +31,7 @@ int main(int argc, char **argv)
     while ((r = fread(buf, 1, sizeof buf, f)) > 0) all.insert(all.end(), buf, buf + r);
     fclose(f);
     size_t o = 0;
-    int rec = 0;
+    int rec = 0, split_mismatch = 0;
     while (o + 4 <= all.size()) {
         uint32_t n;
         memcpy(&n, all.data() + o, 4);
@@ -44,8 +47,23 @@ int main(int argc, char **argv)
             cuo_host::Chains c;
             std::string err;
             double seg = rec % 2 ? 1.0 : 0.5, pre = rec % 2 ? 250.0 : 80.0;
-            bool ok = cuo_host::demux(n ? data : nullptr, n, opt, d, err) && (d.channels == 1 || d.channels == 2) &&
-                      d.granule_match == d.granule_checked && cuo_host::build_chains(d, seg, pre, c, err);
+            bool dm = cuo_host::demux(n ? data : nullptr, n, opt, d, err);
+            cuo_host::Options opt3 = opt;
+            opt3.threads = 3;
+            opt3.range_bytes = 1;
+            cuo_host::Demux d3;
+            std::string err3;
+            bool dm3 = cuo_host::demux(n ? data : nullptr, n, opt3, d3, err3);
+            if (dm != dm3 || err != err3 || d.blob != d3.blob || d.off != d3.off || d.len != d3.len ||
+                d.sample_off != d3.sample_off || d.channels != d3.channels || d.preskip != d3.preskip ||
+                d.toc_total != d3.toc_total || d.last_granule != d3.last_granule || d.play48 != d3.play48 ||
+                d.end_trim != d3.end_trim || d.n_pages != d3.n_pages || d.granule_checked != d3.granule_checked ||
+                d.granule_match != d3.granule_match || d.granule_mismatch != d3.granule_mismatch) {
+                fprintf(stderr, "record %d policy %d: the split demux differs\n", rec, policy);
+                split_mismatch++;
+            }
+            bool ok = dm && (d.channels == 1 || d.channels == 2) && d.granule_match == d.granule_checked &&
+                      cuo_host::build_chains(d, seg, pre, c, err);
             if (ok) {
                 long long keep = 0;
                 for (uint32_t k : c.keep) keep += k;
@@ -59,5 +77,5 @@ int main(int argc, char **argv)
         o += n;
         rec++;
     }
-    return 0;
+    return split_mismatch ? 3 : 0;
 }

@@ -125,8 +125,10 @@ def test_demuxer_on_damaged_streams_under_address_sanitizer(tmp_path):
     AddressSanitizer + UndefinedBehaviorSanitizer and run over 1,500 seeded
     damages of the golden streams, each in a heap buffer of exactly its size,
     under the default options, the page-CRC check and the granule
-    warn-and-resync policy: no report, and under the default options the same
-    streams accepted as by the oracle's port, with the same lengths."""
+    warn-and-resync policy: no report, the demux with its pages split over
+    three threads identical to the one-thread demux in every field, and under
+    the default options the same streams accepted as by the oracle's port, with
+    the same lengths."""
     import json
     import struct
     import sys
