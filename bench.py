@@ -874,7 +874,10 @@ def main():
         import ctypes
         play = [cn.probe_pcm(f) for f in files]
         caps = [p * c for p, c in play]
-        outs = [torch.empty(max(c, 1), dtype=torch.int16, device=dev) for c in caps]
+        # the files' outputs back to back in one device buffer, read back with one copy
+        out_all = torch.empty(max(sum(caps), 1), dtype=torch.int16, device=dev)
+        bounds = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
+        outs = [out_all[int(bounds[i]):int(bounds[i + 1])] for i in range(len(caps))]
         host = torch.empty(max(sum(caps), 1), dtype=torch.int16, pin_memory=True)
         lib = cn.lib()
         n = len(files)
@@ -913,10 +916,7 @@ def main():
                                              err, 512)
             if rc:
                 raise RuntimeError(err.value.decode())
-            o = 0
-            for t_, c in zip(outs, caps):
-                host[o:o + c].copy_(t_[:c], non_blocking=True)
-                o += c
+            host.copy_(out_all, non_blocking=True)
             torch.cuda.synchronize()
 
         for _ in range(2):
