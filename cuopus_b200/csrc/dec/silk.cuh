@@ -874,47 +874,6 @@ DNI void silk_decode_parameters(SilkChan *c, SilkCtrl *ctrl, int condCoding, Sil
 
 // ------------------------------------------------------------------ synthesis
 
-// LPC synthesis of one subframe (the short-term prediction loop of
-// silk/decode_core.c) for an order O known at compile time.  Output i is
-// pres[i] plus the prediction shifted up by 4 (saturating), the prediction
-// being O/2 plus one truncated product per tap on the O previous outputs,
-// summed with wrap-around adds -- so the terms may be summed in any order.
-// Four outputs per step: the taps that read outputs from before the step are
-// summed for all four first (independent of one another), then each output
-// adds the taps on the step's earlier outputs, and the window moves by four.
-// win[15] is the newest output; n is a multiple of 4 (40, 60 or 80).
-template <int O>
-DFN void silk_lpc_synth(int32_t (&win)[16], const int16_t *Acoef, const int32_t *pres, int16_t *pxq, int n,
-                        int32_t Gain_Q10)
-{
-    int32_t a[O];
-#pragma unroll
-    for (int j = 0; j < O; j++) a[j] = Acoef[j];
-    for (int i = 0; i + 4 <= n; i += 4) {
-        int32_t s[4];   // O/2 + the taps of output i + m on outputs before i
-#pragma unroll
-        for (int m = 0; m < 4; m++) {
-            int32_t t = O >> 1;
-#pragma unroll
-            for (int j = m; j < O; j++) t = wadd(t, s_smulwb(win[15 - j + m], a[j]));
-            s[m] = t;
-        }
-        int32_t y[4];
-#pragma unroll
-        for (int m = 0; m < 4; m++) {
-            int32_t p = s[m];
-#pragma unroll
-            for (int j = 0; j < m; j++) p = wadd(p, s_smulwb(y[m - 1 - j], a[j]));
-            y[m] = s_add_sat32(pres[i + m], s_lshift_sat32(p, 4));
-            pxq[i + m] = (int16_t)s_sat16(s_rshift_round(s_smulww(y[m], Gain_Q10), 8));
-        }
-#pragma unroll
-        for (int t = 0; t < 12; t++) win[t] = win[t + 4];
-#pragma unroll
-        for (int m = 0; m < 4; m++) win[12 + m] = y[m];
-    }
-}
-
 // silk/decode_core.c: excitation, LTP and LPC synthesis for one frame
 DNI void silk_decode_core(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *xq, const int16_t *pulses,
                           SilkScratch *w)
@@ -1038,8 +997,32 @@ DNI void silk_decode_core(Lanes L, SilkChan *c, SilkCtrl *ctrl, int16_t *xq, con
         }
         PHASE_END(PH_SILK_LTP, t_ltp, L.id);
         PHASE_BEGIN(t_lpc);
-        if (c->LPC_order == 16) silk_lpc_synth<16>(win, A_Q12, pres, pxq, c->subfr_length, Gain_Q10);
-        else silk_lpc_synth<10>(win, A_Q12, pres, pxq, c->subfr_length, Gain_Q10);
+        // LPC synthesis: order-10/16 recursion per sample.  The prediction is
+        // order/2 plus one truncated product per tap, summed with wrap-around
+        // adds, so the sum may be taken in any order: the taps on samples
+        // older than the newest one are summed while the newest sample is
+        // still being computed, and only tap 0 stays on the recursion's path.
+        const int order = c->LPC_order;
+        int32_t pold = order >> 1;     // order/2 + taps 1.. on the current window
+#pragma unroll
+        for (int j = 1; j < 16; j++)
+            if (j < order) pold = wadd(pold, s_smulwb(win[15 - j], A_Q12[j]));
+        for (int i = 0; i < c->subfr_length; i++) {
+            int32_t p = wadd(pold, s_smulwb(win[15], A_Q12[0]));
+            // taps 1.. of the next sample read win[16 - j]: known already
+            int32_t pa = order >> 1, pb = 0;
+#pragma unroll
+            for (int j = 1; j < 16; j += 2) {
+                if (j < order) pa = wadd(pa, s_smulwb(win[16 - j], A_Q12[j]));
+                if (j + 1 < order) pb = wadd(pb, s_smulwb(win[15 - j], A_Q12[j + 1]));
+            }
+            pold = wadd(pa, pb);
+            int32_t v = s_add_sat32(pres[i], s_lshift_sat32(p, 4));
+#pragma unroll
+            for (int t = 0; t < 15; t++) win[t] = win[t + 1];
+            win[15] = v;
+            pxq[i] = (int16_t)s_sat16(s_rshift_round(s_smulww(v, Gain_Q10), 8));
+        }
         pexc += c->subfr_length;
         pxq += c->subfr_length;
         PHASE_END(PH_SILK_LPC, t_lpc, L.id);

@@ -587,8 +587,29 @@ int choose_width(const Plan &P)
     return t8 < t32 ? 8 : 32;
 }
 
-// H2D of a plan, one decode launch into G.pcm, D2H of the results, validation.
-int run_plan(const Plan &P, cudaStream_t st, Err &err)
+// fn(begin, end) over [0, n) in up to `threads` contiguous ranges, the first
+// on the calling thread.
+template <class F> void run_chunks(int threads, size_t n, F &&fn)
+{
+    size_t t = (size_t)std::max(1, std::min(threads, 64));
+    t = std::min(t, std::max<size_t>(1, n / 256));
+    std::vector<std::thread> pool;
+    for (size_t r = 1; r < t; r++) {
+        size_t a = n * r / t, b = n * (r + 1) / t;
+        try {
+            pool.emplace_back([&fn, a, b] { fn(a, b); });
+        } catch (...) {
+            fn(a, b);   // no thread: run it here
+        }
+    }
+    fn(0, n / t);
+    for (auto &th : pool) th.join();
+}
+
+// H2D of a plan and one decode launch into G.pcm, or into `direct_out` when
+// the caller's outputs are one buffer laid out as the plan's (the decoder
+// writes exactly each chain's kept samples at its offset, nothing else).
+int run_plan(const Plan &P, cudaStream_t st, Err &err, int16_t *direct_out = nullptr)
 {
     int rc;
     uint32_t nch = (uint32_t)P.first.size();
@@ -606,7 +627,7 @@ int run_plan(const Plan &P, cudaStream_t st, Err &err)
     if ((rc = gpu_grow(G.keep, 8ull * nch, err))) return rc;
     if ((rc = gpu_grow(G.out_off, 8ull * nch, err))) return rc;
     if ((rc = gpu_grow(G.res, 16ull * nch, err))) return rc;
-    if ((rc = gpu_grow(G.pcm, 2ull * P.out_elems + 16, err))) return rc;
+    if (!direct_out && (rc = gpu_grow(G.pcm, 2ull * P.out_elems + 16, err))) return rc;
     // stage everything through one pinned buffer, then one async copy per table
     if ((rc = ensure_events(err))) return rc;
     CK(cudaEventRecord(G.evh0, st));
@@ -641,7 +662,7 @@ int run_plan(const Plan &P, cudaStream_t st, Err &err)
     b.trim = (const uint64_t *)G.trim.p;
     b.keep = (const uint64_t *)G.keep.p;
     b.out_off = (const uint64_t *)G.out_off.p;
-    b.out = (int16_t *)G.pcm.p;
+    b.out = direct_out ? direct_out : (int16_t *)G.pcm.p;
     b.res = (uint32_t *)G.res.p;
     b.nchains = (int32_t)nch;
     if ((rc = ensure_occupancy(err))) return rc;
@@ -660,14 +681,16 @@ int run_plan(const Plan &P, cudaStream_t st, Err &err)
     } else {
         const cuo_host::OrderCost oc(cuo_host::order_coefficients(b.width));
         std::vector<double> cost(nch);
-        for (uint32_t c = 0; c < nch; c++) {
-            double s = oc.chain;
-            for (uint32_t k = 0; k < P.npkts[c]; k++) {
-                uint64_t q = (uint64_t)P.first[c] + k;
-                s += oc.of(P.blob.data() + P.off[q], P.len[q], P.chans[c]);
+        run_chunks(env_i("CUOPUS_DEMUX_THREADS", 1), nch, [&](size_t c0, size_t c1) {
+            for (size_t c = c0; c < c1; c++) {
+                double s = oc.chain;
+                for (uint32_t k = 0; k < P.npkts[c]; k++) {
+                    uint64_t q = (uint64_t)P.first[c] + k;
+                    s += oc.of(P.blob.data() + P.off[q], P.len[q], P.chans[c]);
+                }
+                cost[c] = s;
             }
-            cost[c] = s;
-        }
+        });
         std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return cost[x] > cost[y]; });
     }
     b.schedule = 1;
@@ -944,8 +967,15 @@ extern "C" int cuopus_decode_i16_multi(const uint8_t *const *oggs, const size_t 
                            (unsigned long long)need);
         if (need && (!out_devs || !out_devs[f])) return err.set(RC_ARG, "file %d: out_dev is NULL", f);
     }
-    if ((rc = run_plan(P, st, err))) return rc;
-    for (int f = 0; f < nfiles; f++) {
+    // outputs back to back in file order, as the plan lays them out: decode
+    // straight into them; otherwise into the workspace, then one copy per file
+    bool direct = out_devs && out_devs[0] != nullptr;
+    for (int f = 0; f < nfiles && direct; f++) {
+        uint64_t need = P.file_keep[f] * (uint64_t)P.file_chans[f];
+        if (need && out_devs[f] != out_devs[0] + P.file_out0[f]) direct = false;
+    }
+    if ((rc = run_plan(P, st, err, direct ? out_devs[0] : nullptr))) return rc;
+    for (int f = 0; f < nfiles && !direct; f++) {
         uint64_t need = P.file_keep[f] * (uint64_t)P.file_chans[f];
         if (need)
             CK(cudaMemcpyAsync(out_devs[f], (const int16_t *)G.pcm.p + P.file_out0[f], 2 * need,

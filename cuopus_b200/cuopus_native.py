@@ -274,7 +274,9 @@ def decode_ogg_to_f16k_channels(items):
 
 def decode_ogg_to_int16(items, capacities=None):
     """Extension: decode files to 48 kHz interleaved int16 playable PCM (mono or
-    stereo).  Returns a list of (tensor[int16, samples*channels], channels)."""
+    stereo).  Returns a list of (tensor[int16, samples*channels], channels):
+    views of one device buffer holding the files back to back."""
+    import numpy as np
     import torch
     lib = _load()
     blobs = [_as_bytes(x) for x in items]
@@ -286,7 +288,10 @@ def decode_ogg_to_int16(items, capacities=None):
         for b in blobs:
             play, ch = probe_pcm(b)
             capacities.append(play * ch)
-    outs = [torch.empty(max(int(c), 1), dtype=torch.int16, device="cuda") for c in capacities]
+    # one buffer, the files back to back: the library decodes straight into it
+    bounds = np.concatenate([[0], np.cumsum([int(c) for c in capacities])]).astype(np.int64)
+    whole = torch.empty(max(int(bounds[-1]), 1), dtype=torch.int16, device="cuda")
+    outs = [whole[int(bounds[i]):int(bounds[i + 1])] for i in range(n)]
     stream = torch.cuda.current_stream().cuda_stream
     ba = (ctypes.c_char_p * n)(*blobs)
     la = (ctypes.c_size_t * n)(*[len(b) for b in blobs])

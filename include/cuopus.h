@@ -80,7 +80,10 @@ int cuopus_decode_f16k_channels(const uint8_t *const *oggs, const size_t *ns, in
 /* Extension (the reference CLI's int16 "DECODE" output, for mono and stereo):
  * decode N files to 48 kHz interleaved int16 playable PCM.  out_caps are in
  * int16 elements; out_lens receive samples per channel; out_channels (may be
- * NULL) the channel count.  Chains as in cuopus_decode_f16k_on. */
+ * NULL) the channel count.  Chains as in cuopus_decode_f16k_on.  When the
+ * outputs are one buffer with the files back to back in order (out_devs[f] =
+ * out_devs[0] + the play samples x channels of the files before f), the
+ * decoder writes into it directly, with no workspace and no copy. */
 int cuopus_decode_i16_multi(const uint8_t *const *oggs, const size_t *ns, int nfiles, int16_t *const *out_devs,
                             const size_t *out_caps, int64_t *out_lens, int32_t *out_channels, void *cuda_stream,
                             char *errbuf, size_t errcap);

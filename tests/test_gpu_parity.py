@@ -144,6 +144,12 @@ def test_f16k_channels_stereo_and_mono(cuda):
 
 
 def test_i16_stereo_and_mono(cuda):
+    """int16 48 kHz output, mono and stereo, against the CPU pipeline; the
+    outputs back to back in one buffer (decoded in place) and the same outputs
+    in buffers with gaps between them (decoded into the workspace, then
+    copied) hold the same samples."""
+    import ctypes
+    import torch
     from cuopus_b200 import cuopus_native as cn
     streams = _streams("mixed", 4, 3.0, 8300)
     outs = cn.decode_ogg_to_int16(streams)
@@ -151,6 +157,24 @@ def test_i16_stereo_and_mono(cuda):
         want, wch, _ = pipeline.i16(d)
         assert ch == wch
         assert np.array_equal(t.cpu().numpy(), want)
+    caps = [t.numel() for t, _ in outs]
+    gap = 4097
+    big = torch.full((sum(caps) + gap * len(caps),), 7, dtype=torch.int16, device="cuda")
+    starts = [sum(caps[:i]) + gap * (i + 1) for i in range(len(caps))]
+    n = len(streams)
+    lib = cn.lib()
+    err = ctypes.create_string_buffer(512)
+    ol, oc = (ctypes.c_int64 * n)(), (ctypes.c_int32 * n)()
+    rc = lib.cuopus_decode_i16_multi((ctypes.c_char_p * n)(*streams), (ctypes.c_size_t * n)(*map(len, streams)), n,
+                                     (ctypes.c_void_p * n)(*[big.data_ptr() + 2 * s for s in starts]),
+                                     (ctypes.c_size_t * n)(*caps), ol, oc,
+                                     ctypes.c_void_p(torch.cuda.current_stream().cuda_stream), err, 512)
+    assert rc == 0, err.value
+    torch.cuda.synchronize()
+    h = big.cpu().numpy()
+    for i, (t, _) in enumerate(outs):
+        assert np.array_equal(h[starts[i]:starts[i] + caps[i]], t.cpu().numpy())
+        assert np.all(h[starts[i] - gap:starts[i]] == 7)   # the gaps are untouched
 
 
 def _lossy(packets, seed, p_lost, p_dtx):
