@@ -396,101 +396,6 @@ def timed_steps(cn, b, stream, steps):
     return e0.elapsed_time(e1) / steps, kern
 
 
-def sym_capacity(blob, off, lens):
-    """Symbol-log entries reserved per packet: 256 + 8 per byte + 512 per
-    frame (a packet whose log does not fit decodes normally in its chain)."""
-    n = len(lens)
-    lens = lens.astype(np.int64)
-    toc = blob[off.astype(np.int64)].astype(np.int64) if n else np.zeros(0, np.int64)
-    second = blob[np.minimum(off.astype(np.int64) + 1, len(blob) - 1)].astype(np.int64) if n else toc
-    code = toc & 3
-    frames = np.where(code == 0, 1, np.where(code < 3, 2, second & 63))
-    frames = np.where(lens > 0, frames, 0)
-    return 256 + 8 * lens + 512 * frames
-
-
-def two_phase_probe(cn, db, stream, b, args, reps=2):
-    """Diagnostics, untimed: two-phase decoding of the timed batch.  Phase 1
-    decodes every packet on its own (a chain of one packet, one lane per
-    chain, packets ordered by TOC byte so that a warp's lanes take similar
-    packets) recording its symbol log; phase 2 is the tuned launch `b`
-    replaying the logs.  Reports both kernels' times against the normal
-    launch, the log sizes, and whether the output equals the normal decode."""
-    import ctypes
-    import torch
-    h = db.host
-    npk = len(h["len"])
-    dev = stream.device
-    # per-packet channel count (the chain's that covers the packet)
-    pch = np.ones(npk, np.uint8)
-    for c in range(db.n):
-        a = int(h["first"][c])
-        pch[a:a + int(h["npkts"][c])] = h["chans"][c]
-    cap = sym_capacity(h["blob"], h["off"], h["len"])
-    sym_off = np.zeros(npk + 1, np.uint64)
-    sym_off[1:] = np.cumsum(cap)
-    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
-    sym = torch.empty(max(int(sym_off[-1]), 1), dtype=torch.int32, device=dev)
-    sym_off_t = T(sym_off)
-    sym_len = torch.zeros(max(npk, 1), dtype=torch.int32, device=dev)
-    first = T(np.arange(npk, dtype=np.uint32))
-    ones = T(np.ones(npk, np.uint32))
-    chans = T(pch)
-    zeros64 = T(np.zeros(npk, np.uint64))
-    res1 = torch.zeros(4 * max(npk, 1), dtype=torch.int32, device=dev)
-    toc = h["blob"][h["off"].astype(np.int64)].astype(np.int64) if npk else np.zeros(0)
-    order1 = np.ascontiguousarray(np.lexsort((h["len"], toc)).astype(np.uint32))
-    out = {"packets": int(npk), "sym_bytes_reserved": int(sym_off[-1]) * 4}
-    for sched in (0, 1):
-        b1 = cn.Batch()
-        t = db.t
-        b1.data, b1.off, b1.len = t["blob"].data_ptr(), t["off"].data_ptr(), t["len"].data_ptr()
-        b1.first, b1.npkts, b1.channels = first.data_ptr(), ones.data_ptr(), chans.data_ptr()
-        b1.trim, b1.keep, b1.out_off = zeros64.data_ptr(), zeros64.data_ptr(), zeros64.data_ptr()
-        b1.out, b1.res = 0, res1.data_ptr()
-        b1.nchains, b1.width, b1.schedule, b1.max_groups, b1.block = npk, 1, sched, 0, 64
-        b1.order = order1.ctypes.data if sched == 1 else None
-        b1.sym, b1.sym_off, b1.sym_len, b1.sym_mode = sym.data_ptr(), sym_off_t.data_ptr(), sym_len.data_ptr(), 1
-        ms = [cn.decode_batch(b1, stream.cuda_stream) for _ in range(reps)]
-        out["phase1_ms_" + ("static" if sched == 0 else "queue")] = round(min(ms), 2)
-    used = sym_len.cpu().numpy().view(np.uint32)[:npk]
-    good = used != 0xFFFFFFFF
-    out["packets_unlogged"] = int((~good).sum())
-    out["sym_entries_mean"] = round(float(used[good].mean()), 1) if good.any() else 0.0
-    out["sym_entries_max"] = int(used[good].max()) if good.any() else 0
-    out["sym_fill_max"] = round(float((used[good] / cap[good]).max()), 3) if good.any() else 0.0
-    # phase 2 against the normal launch, alternating, same outputs compared
-    b2 = cn.Batch()
-    ctypes.memmove(ctypes.byref(b2), ctypes.byref(b), ctypes.sizeof(b))
-    b2.graph = 0
-    b2.sym, b2.sym_off, b2.sym_len, b2.sym_mode = sym.data_ptr(), sym_off_t.data_ptr(), sym_len.data_ptr(), 2
-    normal, replay = [], []
-    cn.decode_batch(b, stream.cuda_stream)
-    torch.cuda.synchronize()
-    ref_out = db.out.clone()
-    ref_res = db.results().copy()
-    for _ in range(reps):
-        replay.append(cn.decode_batch(b2, stream.cuda_stream))
-        normal.append(cn.decode_batch(b, stream.cuda_stream))
-    cn.decode_batch(b2, stream.cuda_stream)
-    torch.cuda.synchronize()
-    rres = db.results()
-    out["normal_ms"] = round(min(normal), 2)
-    out["phase2_ms"] = round(min(replay), 2)
-    out["replay_equals_normal"] = bool(torch.equal(db.out, ref_out)) and bool(np.array_equal(rres[:, :3],
-                                                                                          ref_res[:, :3]))
-    us = rres[:, 3].astype(np.float64)
-    out["phase2_longest_chain_ms"] = round(float(us.max() / 1e3), 1)
-    out["phase2_chain_seconds"] = round(float(us.sum() / 1e6), 1)
-    out["normal_longest_chain_ms"] = round(float(ref_res[:, 3].max() / 1e3), 1)
-    out["normal_chain_seconds"] = round(float(ref_res[:, 3].astype(np.float64).sum() / 1e6), 1)
-    best1 = min(out["phase1_ms_static"], out["phase1_ms_queue"])
-    out["two_phase_ms"] = round(best1 + out["phase2_ms"], 2)
-    del sym, sym_len, res1
-    torch.cuda.empty_cache()
-    return out
-
-
 def train_cost_model(args, stream):
     """The cost model of the scheduled form, trained (untimed) on another
     corpus than the timed batch (TRAIN_ON): that corpus is decoded once with
@@ -837,9 +742,6 @@ def main():
     ap.add_argument("--budget-gb", type=int, default=40, help="serve: admission budget")
     ap.add_argument("--phases", action="store_true",
                     help="diagnostics, not a bench line: per-stage decoder cycles from libcuopus_phases.so")
-    ap.add_argument("--two-phase", action="store_true",
-                    help="diagnostics after the timed region: two-phase decoding of the batch (record every "
-                         "packet's symbol log, replay it in the chains) against the normal launch")
     ap.add_argument("--fit-order", metavar="INC", default=None,
                     help="not a bench line: fit the file entry points' visiting-order weights on the training "
                          "corpus and write them to INC (cuopus_b200/csrc/ordercost_coef.inc)")
@@ -1054,11 +956,6 @@ def main():
     if rank == 0 and not args.no_parity:
         parity = full_parity(db, threads, e2e_host)
 
-    two_phase = None
-    if args.two_phase and world == 1:
-        two_phase = two_phase_probe(cn, db, stream, b, args)
-        log("two-phase: %s" % json.dumps(two_phase))
-
     cpu = None
     if rank == 0 and world == 1 and args.cpu_budget > 0:
         r, audio, el, used = cpu_decode(files, seg, args.cpu_budget, threads)
@@ -1084,8 +981,6 @@ def main():
                              "kernel": "k_decode_chains"},
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "gpu_launches": args.steps,
                 "decode_errors": bad, "tail": tail, "parity": parity}
-        if two_phase is not None:
-            line["two_phase"] = two_phase
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

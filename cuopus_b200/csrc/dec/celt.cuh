@@ -2156,10 +2156,8 @@ DNI void energy_after_loss(CeltDec *st, int start, int end, int LM)
 
 // celt/celt_decoder.c celt_decode_with_ec_dred (downsample 1, no deep PLC).
 // data == 0 or len <= 1 runs the concealment.  Returns samples or < 0.
-// lg: the packet's symbol log for a frame that brings its own range decoder
-// (dec null: the redundant frames), null for the constant silence frame.
 DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t *pcm, int frame_size,
-                    RangeDec *dec, int accum, CeltScratch *w, SymLog *lg)
+                    RangeDec *dec, int accum, CeltScratch *w)
 {
     const int16_t *eB = T_celt_eBands;
     const int CC = st->channels;
@@ -2186,7 +2184,7 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
     }
     RangeDec _dec;
     if (dec == 0) {
-        rd_init(&_dec, data, len, lg);
+        rd_init(&_dec, data, len);
         dec = &_dec;
     }
     int16_t *oldBandE = st->oldBandE, *oldLogE = st->oldLogE, *oldLogE2 = st->oldLogE2,
@@ -2378,18 +2376,13 @@ DNI int celt_decode(Lanes L, CeltDec *st, const uint8_t *data, int len, int16_t 
     PHASE_BEGIN(t_de);
     deemphasis(L, out_syn[0], out_syn[1], pcm, N, CC, st->preemph_memD, accum);
     PHASE_END(PH_CELT_DEEMPH, t_de, L.id);
-    // the range decoder's final state, read on every lane (it may be a
-    // replayed value, which every lane's log cursor must pass)
-    const uint32_t fin = rd_final(dec);
-    const int tell_end = rd_tell(dec);
-    const int bad = tell_end <= 8 * len && rd_err(dec);
     lead(L, [&]() CUO_INLINE {
-        st->rng = fin;
+        st->rng = dec->rng;
         st->loss_duration = 0;
         st->prefilter_and_fold = 0;
-        if (bad) st->error = 1;
+        if (rd_tell(dec) <= 8 * len && dec->error) st->error = 1;
     });
-    if (tell_end > 8 * len) return -3;   // OPUS_INTERNAL_ERROR
+    if (rd_tell(dec) > 8 * len) return -3;   // OPUS_INTERNAL_ERROR
     return frame_size;
 }
 

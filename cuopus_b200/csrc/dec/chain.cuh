@@ -187,14 +187,10 @@ struct KeepWindow {
 // conceals the same 5760 samples a lost packet always yields but takes the
 // last frame's worth from the next packet's FEC (LBRR) data; the next packet
 // is then decoded normally.
-// sym (may be null): the batch's symbol-log tables (rangedec.cuh).  SYM_RECORD
-// records each packet's log and sets sym->len[p] (SYM_BAD for a packet whose
-// log overflowed or whose decode failed); SYM_REPLAY replays every packet
-// whose log is good and decodes the rest normally.
 DNI void decode_chain(Lanes L, ChainSlot *slot, const uint8_t *data, const uint64_t *off,
                       const uint32_t *len, uint32_t first, uint32_t npkts, int channels, int16_t *out,
                       uint64_t trim, uint64_t keep, uint32_t *pkt_nsamp, uint32_t *pkt_rng, ChainResult *res,
-                      PacketStage *stage, int fec, const SymArgs *sym)
+                      PacketStage *stage, int fec)
 {
     OpusDec *st = &slot->dec;
     opus_init(st, channels);
@@ -231,19 +227,8 @@ DNI void decode_chain(Lanes L, ChainSlot *slot, const uint8_t *data, const uint6
             pk = data + off[p + 1];
             n = (int32_t)len[p + 1];
         }
-        SymLog lg;   // this lane's cursor over the packet's symbol log
-        SymLog *lgp = nullptr;
-        if (sym && !use_fec && (sym->mode == SYM_RECORD || sym->len[p] != SYM_BAD)) {
-            lg.base = sym->base + sym->off[p];
-            lg.cap = (uint32_t)(sym->off[p + 1] - sym->off[p]);
-            lg.pos = 0;
-            lg.mode = sym->mode;
-            lg.overflow = 0;
-            lgp = &lg;
-        }
-        int ret = opus_decode_packet(L, st, pk, n, slot->frame_buf, &slot->scratch, win, use_fec, lgp);
+        int ret = opus_decode_packet(L, st, pk, n, slot->frame_buf, &slot->scratch, win, use_fec);
         PHASE_END(PH_PACKET, t_pk, L.id);
-        if (lgp && lg.mode == SYM_RECORD && L.id == 0) sym->len[p] = (ret < 0 || lg.overflow) ? SYM_BAD : lg.pos;
         lsync(L);   // every lane is done with this packet's buffer before it is refilled
         if (ret < 0) {
             stop = ret;

@@ -191,15 +191,13 @@ DNI void smooth_fade(Lanes L, const int16_t *in1, const int16_t *in2, int16_t *o
 // src/opus_decoder.c opus_decode_frame (:237-668).  D is the recursion depth;
 // fec = 1 decodes the SILK layer's in-band FEC (LBRR) frames of `data` and
 // conceals the CELT layer.
-// lg: the packet's symbol log (null: none).
 template <int D>
 DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16_t *pcm, int frame_size,
-                   OpusScratch *w, int fec, SymLog *lg)
+                   OpusScratch *w, int fec)
 {
     const int F20 = 960, F10 = 480, F5 = 240, F2_5 = 120;
     const int C = st->channels;
     RangeDec dec;
-    dec.lg = nullptr;
     int silk_ret = 0, celt_ret = 0;
     int audiosize, mode, bandwidth;
     int transition = 0, redundancy = 0, redundancy_bytes = 0, celt_to_silk = 0;
@@ -215,7 +213,7 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
         audiosize = st->frame_size;
         mode = st->mode;
         bandwidth = st->bandwidth;
-        rd_init(&dec, data, (uint32_t)len, lg);
+        rd_init(&dec, data, (uint32_t)len);
     } else {
         audiosize = frame_size;
         mode = st->prev_redundancy ? MODE_CELT_ONLY : st->prev_mode;
@@ -228,7 +226,7 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
         if (audiosize > F20) {
             if constexpr (D == 0) {
                 do {
-                    int ret = opus_frame<1>(L, st, 0, 0, pcm, imin(audiosize, F20), w, 0, nullptr);
+                    int ret = opus_frame<1>(L, st, 0, 0, pcm, imin(audiosize, F20), w, 0);
                     if (ret < 0) return ret;
                     pcm += ret * C;
                     audiosize -= ret;
@@ -250,7 +248,7 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
     if (transition && mode == MODE_CELT_ONLY) {
         if constexpr (D == 0) {
             pcm_transition = w->pcm_transition;
-            opus_frame<1>(L, st, 0, 0, pcm_transition, imin(F5, audiosize), w, 0, nullptr);
+            opus_frame<1>(L, st, 0, 0, pcm_transition, imin(F5, audiosize), w, 0);
         }
     }
     if (audiosize > frame_size) return OPUS_BAD_ARG;
@@ -306,9 +304,7 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
             redundancy_bytes = mode == MODE_HYBRID ? (int32_t)rd_uint(&dec, 256) + 2
                                                    : len - ((rd_tell(&dec) + 7) >> 3);
             len -= redundancy_bytes;
-            // (the second and third tests never hold for a decoded tell; they
-            // keep a replayed symbol log that fell out of step inside the packet)
-            if (len * 8 < rd_tell(&dec) || len < 0 || redundancy_bytes < 0) {
+            if (len * 8 < rd_tell(&dec)) {
                 len = 0;
                 redundancy_bytes = 0;
                 redundancy = 0;
@@ -321,7 +317,7 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
     if (transition && mode != MODE_CELT_ONLY) {
         if constexpr (D == 0) {
             pcm_transition = w->pcm_transition;
-            opus_frame<1>(L, st, 0, 0, pcm_transition, imin(F5, audiosize), w, 0, nullptr);
+            opus_frame<1>(L, st, 0, 0, pcm_transition, imin(F5, audiosize), w, 0);
         }
     }
     int16_t *redundant_audio = w->redundant_audio;
@@ -341,7 +337,7 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
         if (redundancy && celt_to_silk) st->celt.start = 0;
     });
     if (redundancy && celt_to_silk) {
-        celt_decode(L, &st->celt, data + len, redundancy_bytes, redundant_audio, F5, 0, 0, &w->celt, lg);
+        celt_decode(L, &st->celt, data + len, redundancy_bytes, redundant_audio, F5, 0, 0, &w->celt);
         redundant_rng = st->celt.rng;
     }
     // the previous mode decides the CELT reset and the hybrid -> SILK silence
@@ -357,15 +353,15 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
     if (mode != MODE_SILK_ONLY) {
         int celt_frame_size = imin(F20, frame_size);
         celt_ret = celt_decode(L, &st->celt, fec ? 0 : data, len, pcm, celt_frame_size, (data && !fec) ? &dec : 0,
-                               celt_accum, &w->celt, nullptr);
+                               celt_accum,
+                               &w->celt);
     } else {
         const uint8_t silence[2] = {0xFF, 0xFF};
         if (!celt_accum) {
             LFOR(L, i, 0, frame_size * C) pcm[i] = 0;
             lsync(L);
         }
-        // a constant frame whose decode depends on the previous packet: never logged
-        if (silence_frame) celt_decode(L, &st->celt, silence, 2, pcm, F2_5, 0, celt_accum, &w->celt, nullptr);
+        if (silence_frame) celt_decode(L, &st->celt, silence, 2, pcm, F2_5, 0, celt_accum, &w->celt);
     }
     if (mode != MODE_CELT_ONLY && !celt_accum) {
         LFOR(L, i, 0, frame_size * C) pcm[i] = c_sat16((int32_t)pcm[i] + pcm_silk[i]);
@@ -376,7 +372,7 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
             celt_reset(&st->celt);
             st->celt.start = 0;
         });
-        celt_decode(L, &st->celt, data + len, redundancy_bytes, redundant_audio, F5, 0, 0, &w->celt, lg);
+        celt_decode(L, &st->celt, data + len, redundancy_bytes, redundant_audio, F5, 0, 0, &w->celt);
         redundant_rng = st->celt.rng;
         smooth_fade(L, pcm + C * (frame_size - F2_5), redundant_audio + C * F2_5, pcm + C * (frame_size - F2_5),
                     F2_5, C);
@@ -397,10 +393,9 @@ DNI int opus_frame(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16
     // test builds only: which branches of the frame decode ran
     if (L.id == 0) cuo_frame_event(D, mode, prev_mode, redundancy, celt_to_silk, transition, silence_frame);
 #endif
-    // read on every lane: a replayed value passes every lane's log cursor
-    const uint32_t final_rng = len <= 1 ? 0u : rd_final(&dec) ^ redundant_rng;
     lead(L, [&]() CUO_INLINE {
-        st->rangeFinal = final_rng;
+        if (len <= 1) st->rangeFinal = 0;
+        else st->rangeFinal = dec.rng ^ redundant_rng;
         st->prev_mode = mode;
         st->prev_redundancy = redundancy && !celt_to_silk;
     });
@@ -429,7 +424,7 @@ DNI int conceal_samples(Lanes L, OpusDec *st, int n, int16_t *frame_buf, OpusScr
 {
     int pcm_count = 0;
     do {
-        int ret = opus_frame<0>(L, st, 0, 0, frame_buf, n - pcm_count, w, 0, nullptr);
+        int ret = opus_frame<0>(L, st, 0, 0, frame_buf, n - pcm_count, w, 0);
         if (ret < 0) return ret;
         emit(frame_buf, ret);
         pcm_count += ret;
@@ -467,7 +462,7 @@ DNI int decode_fec(Lanes L, OpusDec *st, const uint8_t *data, int size0, int pac
         st->frame_size = packet_frame_size;
         st->stream_channels = packet_stream_channels;
     });
-    int ret = opus_frame<0>(L, st, data, size0, frame_buf, packet_frame_size, w, 1, nullptr);
+    int ret = opus_frame<0>(L, st, data, size0, frame_buf, packet_frame_size, w, 1);
     if (ret < 0) return ret;
     emit(frame_buf, ret);
     lead(L, [&]() CUO_INLINE { st->last_packet_duration = frame_size; });
@@ -480,11 +475,10 @@ DNI int decode_fec(Lanes L, OpusDec *st, const uint8_t *data, int size0, int pac
 // frame buffer is reused for the next frame.  fec = 1 is decode_fec = 1: the
 // packet is the one after a lost packet, and the lost packet's audio is
 // concealed up to the last frame, which comes from the packet's FEC data
-// (:745-779).  lg: the packet's symbol log (null: decode without one; FEC
-// decodes never use one).
+// (:745-779).
 template <class Emit>
 DFN int opus_decode_packet(Lanes L, OpusDec *st, const uint8_t *data, int32_t len, int16_t *frame_buf,
-                           OpusScratch *w, Emit &emit, int fec, SymLog *lg = nullptr)
+                           OpusScratch *w, Emit &emit, int fec)
 {
     const int frame_size = MAX_PACKET_SAMPLES;
     if (len == 0 || data == 0) {
@@ -515,7 +509,7 @@ DFN int opus_decode_packet(Lanes L, OpusDec *st, const uint8_t *data, int32_t le
     });
     int nb_samples = 0;
     for (int i = 0; i < count; i++) {
-        int ret = opus_frame<0>(L, st, data, size[i], frame_buf, frame_size - nb_samples, w, 0, lg);
+        int ret = opus_frame<0>(L, st, data, size[i], frame_buf, frame_size - nb_samples, w, 0);
         if (ret < 0) return ret;
         emit(frame_buf, ret);
         data += size[i];

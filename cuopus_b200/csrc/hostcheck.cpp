@@ -54,7 +54,6 @@ struct hc_job {
     cuo::ChainResult *res;
     int nchains;
     int fec;
-    const cuo::SymArgs *sym;
     int next;
     pthread_mutex_t mu;
 };
@@ -77,7 +76,7 @@ static void *hc_worker(void *arg)
         cuo::decode_chain(L, slot, j->data, j->off, j->len, j->first[c], j->npkts[c], j->channels[c],
                           j->pcm ? j->pcm + j->pcm_off[c] : nullptr, j->trim ? j->trim[c] : 0,
                           j->keep ? j->keep[c] : (uint64_t)-1 / 4, j->pkt_nsamp ? j->pkt_nsamp + r : nullptr,
-                          j->pkt_rng ? j->pkt_rng + r : nullptr, &j->res[c], nullptr, j->fec, j->sym);
+                          j->pkt_rng ? j->pkt_rng + r : nullptr, &j->res[c], nullptr, j->fec);
     }
     free(slot);
     return nullptr;
@@ -85,17 +84,12 @@ static void *hc_worker(void *arg)
 
 // Same layout as the oracle's oref_decode_chains, plus per-chain channels and
 // keep windows (trim/keep may be null: keep everything).  res: 4 words per chain.
-// sym_mode 1 / 2: record / replay the packets' symbol logs (sym_off: npackets
-// + 1 entry offsets into sym; sym_len: per packet, written when recording).
-int hc_decode_chains_sym(const uint8_t *data, const uint64_t *off, const uint32_t *len, const uint32_t *first,
+int hc_decode_chains_fec(const uint8_t *data, const uint64_t *off, const uint32_t *len, const uint32_t *first,
                          const uint32_t *npkts, const int32_t *channels, int nchains, int16_t *pcm,
                          const uint64_t *pcm_off, const uint64_t *trim, const uint64_t *keep, const uint64_t *rec_off,
-                         uint32_t *pkt_nsamp, uint32_t *pkt_rng, void *res, int nthreads, int fec, uint32_t *sym,
-                         const uint64_t *sym_off, uint32_t *sym_len, int sym_mode)
+                         uint32_t *pkt_nsamp, uint32_t *pkt_rng, void *res, int nthreads, int fec)
 {
-    cuo::SymArgs sa{sym, sym_off, sym_len, sym_mode};
     hc_job j;
-    j.sym = sym_mode ? &sa : nullptr;
     j.fec = fec;
     j.data = data; j.off = off; j.len = len; j.first = first; j.npkts = npkts; j.channels = channels;
     j.pcm = pcm; j.pcm_off = pcm_off; j.trim = trim; j.keep = keep; j.rec_off = rec_off;
@@ -114,15 +108,6 @@ int hc_decode_chains_sym(const uint8_t *data, const uint64_t *off, const uint32_
     for (int t = 0; t < started; t++) pthread_join(th[t], nullptr);
     pthread_mutex_destroy(&j.mu);
     return 0;
-}
-
-int hc_decode_chains_fec(const uint8_t *data, const uint64_t *off, const uint32_t *len, const uint32_t *first,
-                         const uint32_t *npkts, const int32_t *channels, int nchains, int16_t *pcm,
-                         const uint64_t *pcm_off, const uint64_t *trim, const uint64_t *keep, const uint64_t *rec_off,
-                         uint32_t *pkt_nsamp, uint32_t *pkt_rng, void *res, int nthreads, int fec)
-{
-    return hc_decode_chains_sym(data, off, len, first, npkts, channels, nchains, pcm, pcm_off, trim, keep, rec_off,
-                                pkt_nsamp, pkt_rng, res, nthreads, fec, nullptr, nullptr, nullptr, 0);
 }
 
 int hc_decode_chains(const uint8_t *data, const uint64_t *off, const uint32_t *len, const uint32_t *first,
@@ -368,7 +353,7 @@ int hc_celt_frames(const uint8_t *data, const uint32_t *lens, int frames, int C,
     size_t off = 0;
     for (int f = 0; f < frames; f++) {
         int ret = cuo::celt_decode(L, &st, lens[f] ? data + off : nullptr, (int)lens[f], out + (size_t)f * N * C, N,
-                                   nullptr, 0, &w, nullptr);
+                                   nullptr, 0, &w);
         rng[f] = ret < 0 ? (uint32_t)ret : st.rng;
         off += lens[f];
     }

@@ -45,7 +45,6 @@ struct DecodeArgs {
     int stage;                  // packets staged in shared memory (STAGE_BYTES per group)
     int scalar;                 // one active lane per group (the reference kernel's slot layout)
     int fec;                    // in-band FEC for lost packets (decode_chain)
-    SymArgs sym;                // symbol logs of two-phase decoding (mode 0: off)
     // Tail scheduling (queue schedule, light_sms > 0): the warps of SMs whose id
     // is below light_sms keep only light_warps of themselves and take the
     // first long_chains positions of the order first; every other SM keeps
@@ -160,8 +159,7 @@ __global__ void __launch_bounds__(128, CUO_MIN_BLOCKS) k_decode_chains(DecodeArg
         decode_chain(L, slot, a.data, a.off, a.len, a.first[c], a.npkts[c], a.channels[c],
                      a.out ? a.out + a.out_off[c] : nullptr, a.trim[c], a.keep[c],
                      a.pkt_nsamp ? a.pkt_nsamp + a.rec_off[c] : nullptr,
-                     a.pkt_rng ? a.pkt_rng + a.rec_off[c] : nullptr, &a.res[c], stage, a.fec,
-                     a.sym.mode ? &a.sym : nullptr);
+                     a.pkt_rng ? a.pkt_rng + a.rec_off[c] : nullptr, &a.res[c], stage, a.fec);
         unsigned long long us = (globaltimer_ns() - t0) / 1000ull;
         if (L.id == 0) a.res[c].time_us = (uint32_t)(us < 1 ? 1 : us > 0xffffffffull ? 0xffffffffull : us);
     }

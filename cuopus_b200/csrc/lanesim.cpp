@@ -71,7 +71,6 @@ struct LaneSim {
     uint32_t *pkt_nsamp, *pkt_rng;
     ChainResult *res;
     int fec;
-    const SymArgs *sym;
     // hazard detector (barrier-only schedule): the slot as the barrier released
     // (s0) and as the previous lane arrived (sp)
     int detect;
@@ -248,8 +247,7 @@ NOINSTR static void sim_lane_main(unsigned lo, unsigned hi, int id)
     L.sim = s;
     s->busy = 0;
     decode_chain(L, s->slot, s->data, s->off, s->len, s->first, s->npkts, s->channels, s->out, s->trim, s->keep,
-                 L.id == 0 ? s->pkt_nsamp : nullptr, L.id == 0 ? s->pkt_rng : nullptr, s->res, nullptr, s->fec,
-                 s->sym);
+                 L.id == 0 ? s->pkt_nsamp : nullptr, L.id == 0 ? s->pkt_rng : nullptr, s->res, nullptr, s->fec);
     s->busy = 1;
     s->state[id] = FINISHED;
     int left = 0;
@@ -315,7 +313,6 @@ struct ls_job {
     uint32_t *pkt_nsamp, *pkt_rng;
     cuo::ChainResult *res;
     int nchains, width, max_run, fec, detect;
-    const cuo::SymArgs *sym;
     uint64_t seed;
     unsigned long long switches, hazards;
     int next;
@@ -338,7 +335,6 @@ NOINSTR static void *ls_worker(void *arg)
         s->off = j->off;
         s->len = j->len;
         s->fec = j->fec;
-        s->sym = j->sym;
         s->detect = j->max_run == 0 && j->detect;
         if (s->detect) {
             s->s0 = (unsigned char *)malloc(sizeof(cuo::ChainSlot));
@@ -390,22 +386,16 @@ NOINSTR static void *ls_worker(void *arg)
 // count goes to *hazards (may be null) and the first hazard of each chain is
 // reported on stderr with the code locations of the stretch's two barriers.
 // Returns the number of lane switches made, or -1 on bad arguments.
-// ls_decode_chains_sym: the same with the packets' symbol logs replayed
-// (sym_mode 2; sym_off: npackets + 1 entry offsets into sym, sym_len: entries
-// per packet as the record pass left them) or recorded (sym_mode 1).
-NOINSTR long long ls_decode_chains_sym(const uint8_t *data, const uint64_t *off, const uint32_t *len,
-                                       const uint32_t *first, const uint32_t *npkts, const int32_t *channels,
-                                       int nchains, int16_t *pcm, const uint64_t *pcm_off, const uint64_t *trim,
-                                       const uint64_t *keep, const uint64_t *rec_off, uint32_t *pkt_nsamp,
-                                       uint32_t *pkt_rng, void *res, int nthreads, int fec, int width, int max_run,
-                                       uint64_t seed, int detect, unsigned long long *hazards, uint32_t *sym,
-                                       const uint64_t *sym_off, uint32_t *sym_len, int sym_mode)
+NOINSTR long long ls_decode_chains(const uint8_t *data, const uint64_t *off, const uint32_t *len,
+                                   const uint32_t *first, const uint32_t *npkts, const int32_t *channels,
+                                   int nchains, int16_t *pcm, const uint64_t *pcm_off, const uint64_t *trim,
+                                   const uint64_t *keep, const uint64_t *rec_off, uint32_t *pkt_nsamp,
+                                   uint32_t *pkt_rng, void *res, int nthreads, int fec, int width, int max_run,
+                                   uint64_t seed, int detect, unsigned long long *hazards)
 {
     if (width < 1 || width > cuo::SIM_MAX_LANES || (width & (width - 1)) || max_run < 0) return -1;
-    cuo::SymArgs sa{sym, sym_off, sym_len, sym_mode};
     ls_job j;
     memset(&j, 0, sizeof j);
-    j.sym = sym_mode ? &sa : nullptr;
     j.data = data; j.off = off; j.len = len; j.first = first; j.npkts = npkts; j.channels = channels;
     j.pcm = pcm; j.pcm_off = pcm_off; j.trim = trim; j.keep = keep; j.rec_off = rec_off;
     j.pkt_nsamp = pkt_nsamp; j.pkt_rng = pkt_rng; j.res = (cuo::ChainResult *)res;
@@ -424,18 +414,6 @@ NOINSTR long long ls_decode_chains_sym(const uint8_t *data, const uint64_t *off,
     pthread_mutex_destroy(&j.mu);
     if (hazards) *hazards = j.hazards;
     return (long long)j.switches;
-}
-
-NOINSTR long long ls_decode_chains(const uint8_t *data, const uint64_t *off, const uint32_t *len,
-                                   const uint32_t *first, const uint32_t *npkts, const int32_t *channels,
-                                   int nchains, int16_t *pcm, const uint64_t *pcm_off, const uint64_t *trim,
-                                   const uint64_t *keep, const uint64_t *rec_off, uint32_t *pkt_nsamp,
-                                   uint32_t *pkt_rng, void *res, int nthreads, int fec, int width, int max_run,
-                                   uint64_t seed, int detect, unsigned long long *hazards)
-{
-    return ls_decode_chains_sym(data, off, len, first, npkts, channels, nchains, pcm, pcm_off, trim, keep, rec_off,
-                                pkt_nsamp, pkt_rng, res, nthreads, fec, width, max_run, seed, detect, hazards,
-                                nullptr, nullptr, nullptr, 0);
 }
 
 }

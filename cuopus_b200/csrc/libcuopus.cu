@@ -390,15 +390,6 @@ int decode_batch(const cuopus_batch *b, cudaStream_t st, float *kernel_ms, Err &
     a.use_queue = b->schedule == 1;
     a.scalar = b->scalar != 0;
     a.fec = b->fec != 0;
-    if (b->sym_mode) {
-        if (b->sym_mode != cuo::SYM_RECORD && b->sym_mode != cuo::SYM_REPLAY)
-            return err.set(RC_ARG, "sym_mode %d: 0, 1 (record) or 2 (replay)", b->sym_mode);
-        if (!b->sym || !b->sym_off || !b->sym_len) return err.set(RC_ARG, "sym_mode set without its tables");
-        a.sym.base = b->sym;
-        a.sym.off = b->sym_off;
-        a.sym.len = b->sym_len;
-        a.sym.mode = b->sym_mode;
-    }
     if (tail) {
         int gpw = 32 / width;
         a.sm_rank = (unsigned *)G.queue.p + 2;

@@ -52,8 +52,7 @@ class Batch(ctypes.Structure):
                 ("width", ctypes.c_int32), ("schedule", ctypes.c_int32), ("max_groups", ctypes.c_int32),
                 ("order", ctypes.c_void_p), ("block", ctypes.c_int32), ("graph", ctypes.c_int32),
                 ("scalar", ctypes.c_int32), ("fec", ctypes.c_int32), ("light_sms", ctypes.c_int32),
-                ("long_chains", ctypes.c_int32), ("sym", ctypes.c_void_p), ("sym_off", ctypes.c_void_p),
-                ("sym_len", ctypes.c_void_p), ("sym_mode", ctypes.c_int32)]
+                ("long_chains", ctypes.c_int32)]
 
 
 _lib = None

@@ -139,22 +139,6 @@ typedef struct cuopus_batch {
                             runs max_groups / SMs warps (all resident if max_groups is 0).  The
                             launch grid is then every resident group. */
     int32_t long_chains;
-    /* Two-phase decoding (0 = off).  The range decoder's output for a packet
-     * does not depend on earlier packets, so each packet can be decoded once on
-     * its own, in parallel with all others, recording what the range decoder
-     * hands the decoder (sym_mode 1: a batch whose chains are single packets,
-     * out NULL), and the chains then decoded replaying it (sym_mode 2: the
-     * range coder's arithmetic leaves the chain's serial path).  sym: device
-     * uint32 entries; sym_off: npackets + 1 offsets, packet p's entries are
-     * sym[sym_off[p] .. sym_off[p + 1]); sym_len: per packet, written by the
-     * record pass (entries used, or 0xFFFFFFFF when they did not fit or the
-     * packet failed to decode) and read by the replay pass, which decodes such
-     * packets normally.  FEC decodes never use the log.  Decoded samples are
-     * the same with or without it. */
-    uint32_t *sym;
-    const uint64_t *sym_off;
-    uint32_t *sym_len;
-    int32_t sym_mode;
 } cuopus_batch;
 
 int cuopus_decode_batch(const cuopus_batch *b, void *cuda_stream, float *kernel_ms, char *errbuf, size_t errcap);
