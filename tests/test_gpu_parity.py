@@ -329,3 +329,30 @@ def test_tail_scheduling_keeps_the_bits(cuda):
             assert int(res[s, 0]) == 0 and int(res[s, 1]) == int(ref["samples"][0])
             o = int(meta["out_off"][s])
             assert np.array_equal(out[o:o + int(meta["keep"][s]) * nch[s]], ref["pcm"][0]), (light, s)
+
+
+@pytest.mark.gpu
+def test_visiting_order_keeps_the_bits(cuda, monkeypatch):
+    """The file entry points' chain order (fitted additive cost, or decoded
+    samples with CUOPUS_ORDER=samples) changes no sample: int16 at 32 lanes
+    per chain (whole streams) and f16k at 8 (1 s chains of a long stream)."""
+    from cuopus_b200 import cuopus_native as cn
+    streams = _streams("mixed", 6, 4.0, 8600)
+    long_one = corpus.make_stream(dict(kind="mixed", seed=8700, seconds=20.0, channels=1))
+    got = {}
+    for order in (None, "samples"):
+        if order:
+            monkeypatch.setenv("CUOPUS_ORDER", order)
+        else:
+            monkeypatch.delenv("CUOPUS_ORDER", raising=False)
+        monkeypatch.setenv("CUOPUS_SEG_S", "1e9")
+        monkeypatch.delenv("CUOPUS_STRIDE", raising=False)
+        i16 = [t.cpu().numpy() for t, _ in cn.decode_ogg_to_int16(streams)]
+        monkeypatch.setenv("CUOPUS_SEG_S", "1.0")
+        monkeypatch.setenv("CUOPUS_STRIDE", "8")
+        f16 = cn.decode_ogg_to_cuda_tensor(long_one).cpu().numpy()
+        got[order] = (i16, f16, cn.last_stats()["width"])
+    a, b = got[None], got["samples"]
+    assert all(np.array_equal(x, y) for x, y in zip(a[0], b[0]))
+    assert np.array_equal(a[1], b[1])
+    assert a[2] == b[2] == 8
