@@ -590,6 +590,12 @@ def serve_bench(args, files, dev):
             wall = max(done_at)
             served = {"value": total_audio / wall, "p50_ms": float(np.percentile(lat, 50)),
                       "p99_ms": float(np.percentile(lat, 99)), "wall_s": wall}
+            if args.serve_no_plain:
+                out["rates"][str(int(rate))] = {"offered_audio_s_per_s": total_audio / float(arrivals[-1]),
+                                                "served": served}
+                log("serve %g/s: served %.0f audio-s/s p50 %.0f p99 %.0f ms" % (rate, served["value"],
+                                                                             served["p50_ms"], served["p99_ms"]))
+                continue
             # one launch per request, arrival order, one at a time
             lat2 = []
             t0 = time.perf_counter()
@@ -740,6 +746,8 @@ def main():
     ap.add_argument("--serve-width", type=int, default=8, help="serve: lanes per chain of the server")
     ap.add_argument("--serve-inflight", type=int, default=8, help="serve: decode waves in flight")
     ap.add_argument("--budget-gb", type=int, default=40, help="serve: admission budget")
+    ap.add_argument("--serve-no-plain", action="store_true",
+                    help="serve: skip the one-launch-per-request comparison (development sweeps)")
     ap.add_argument("--phases", action="store_true",
                     help="diagnostics, not a bench line: per-stage decoder cycles from libcuopus_phases.so")
     ap.add_argument("--fit-order", metavar="INC", default=None,
