@@ -59,8 +59,12 @@ enum { SM_RANK_SLOTS = 256 };
 
 // Shared memory a block of `block` threads at `width` lanes per chain uses for
 // packet staging; 0 (no staging) when it would exceed 48 KB per block.
+// Packet staging takes shared memory from the SM's unified L1 / shared
+// storage; CUOPUS_STAGE=0 turns it off (all of that storage stays L1).
 inline int stage_smem_bytes(int block, int width)
 {
+    const char *e = getenv("CUOPUS_STAGE");
+    if (e && e[0] == '0' && e[1] == 0) return 0;
     int bytes = (block / width) * (int)STAGE_BYTES;
     return bytes <= 48 * 1024 ? bytes : 0;
 }

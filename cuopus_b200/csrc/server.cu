@@ -619,6 +619,21 @@ extern "C" int cuopus_server_wait(cuopus_server *s, uint64_t id, int64_t timeout
     return rc;
 }
 
+extern "C" int cuopus_server_request_size(cuopus_server *s, uint64_t id, int64_t *out_samples,
+                                          int32_t *channels, size_t *out_bytes)
+{
+    if (!s) return 3;
+    std::lock_guard<std::mutex> g(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return 3;
+    const Request *r = it->second.get();
+    int64_t n = s->cfg.f16k ? r->n16 : (int64_t)r->keep_total;
+    if (out_samples) *out_samples = n;
+    if (channels) *channels = r->d.channels;
+    if (out_bytes) *out_bytes = s->cfg.f16k ? 4 * (size_t)r->n16 : 2 * (size_t)r->keep_total * (size_t)r->d.channels;
+    return 0;
+}
+
 extern "C" int cuopus_server_get_stats(cuopus_server *s, cuopus_server_stats *st)
 {
     if (!s || !st) return 3;

@@ -46,9 +46,12 @@ def _lib():
                                            ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32),
                                            ctypes.POINTER(ctypes.c_double)] + tail
         lib.cuopus_server_get_stats.argtypes = [c_p, ctypes.POINTER(ServerStats)]
+        lib.cuopus_server_request_size.argtypes = [c_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int64),
+                                                   ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_size_t)]
         lib.cuopus_server_destroy.argtypes = [c_p]
         lib.cuopus_server_destroy.restype = None
-        for f in ("cuopus_server_create", "cuopus_server_submit", "cuopus_server_wait", "cuopus_server_get_stats"):
+        for f in ("cuopus_server_create", "cuopus_server_submit", "cuopus_server_wait", "cuopus_server_get_stats",
+                  "cuopus_server_request_size"):
             getattr(lib, f).restype = ctypes.c_int
         lib._srv_bound = True
     return lib
@@ -75,11 +78,12 @@ class Server:
         rc = _lib().cuopus_server_submit(self._h, data, len(data), ctypes.byref(rid), err, 512)
         if rc:
             raise cn.CuopusError(rc, err.value.decode(errors="replace"))
-        if self.f16k:
-            self._sizes[rid.value] = 4 * max(cn.probe(data), 1)
-        else:
-            play, ch = cn.probe_pcm(data)
-            self._sizes[rid.value] = 2 * max(play * ch, 1)
+        # the output size, from the server's own demux of the request
+        nbytes = ctypes.c_size_t(0)
+        rc = _lib().cuopus_server_request_size(self._h, rid.value, None, None, ctypes.byref(nbytes))
+        if rc:
+            raise cn.CuopusError(rc, "request %d: no size" % rid.value)
+        self._sizes[rid.value] = max(int(nbytes.value), 4)
         return rid.value
 
     def wait(self, rid, timeout_ms=-1):
@@ -94,7 +98,7 @@ class Server:
                                        ctypes.byref(n), ctypes.byref(ch), ctypes.byref(lat), err, 512)
         if rc:
             raise cn.CuopusError(rc, err.value.decode(errors="replace"))
-        # the buffer was sized from the probe, so the view is the whole output
+        # the buffer was sized from the server's demux, so the view is the whole output
         if self.f16k:
             out = buf[:4 * n.value].view(np.float32)
         else:

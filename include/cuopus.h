@@ -282,6 +282,11 @@ int cuopus_server_submit(cuopus_server *s, const uint8_t *ogg, size_t n, uint64_
 int cuopus_server_wait(cuopus_server *s, uint64_t id, int64_t timeout_ms, void *host_out, size_t out_cap_bytes,
                        int64_t *out_samples, int32_t *channels, double *latency_ms, char *errbuf, size_t errcap);
 int cuopus_server_get_stats(cuopus_server *s, cuopus_server_stats *st);
+/* Output size of a submitted request, known from its demux at submit: samples
+ * per channel (int16) or 16 kHz samples (f16k), the channel count, and the
+ * bytes cuopus_server_wait writes.  RC 3 for an unknown id. */
+int cuopus_server_request_size(cuopus_server *s, uint64_t id, int64_t *out_samples, int32_t *channels,
+                               size_t *out_bytes);
 /* Finish admitted work, drop queued requests, free everything. */
 void cuopus_server_destroy(cuopus_server *s);
 
