@@ -25,10 +25,25 @@
 
 namespace cuo {
 
+// Two instances of the decoder kernel.  Groups of 8 lanes or fewer put 4 or
+// more chains in each warp, and throughput is what such launches are for (1 s
+// chains of long files, the server's waves): they run the instance compiled
+// for 3 resident 128-thread blocks (at most 170 registers, so 12 warps per SM
+// at 64-thread blocks instead of 8), whose chains each decode slower (spills)
+// but more of them are in flight: the 2 h file in 1 s chains at 8 lanes,
+// 179-180 ms against 188-189 (same box, alternating).  Wider groups decode the
+// long chains that set an uneven batch's step, with few warps per SM: they
+// run the instance with the full register budget (255), which decodes each
+// chain faster (the mixed batch at 5 warps per SM: 2,401-2,496 ms against
+// 2,798-2,803 with the register cap).
+static bool dense_instance(int width) { return width <= 8; }
+
 cudaError_t decode_kernel_occupancy(int block, int width, int *blocks_per_sm)
 {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_decode_chains, block,
-                                                         (size_t)stage_smem_bytes(block, width));
+    size_t smem = (size_t)stage_smem_bytes(block, width);
+    if (dense_instance(width))
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_decode_chains<3>, block, smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_decode_chains<1>, block, smem);
 }
 
 cudaError_t decode_kernel_launch(const DecodeArgs &a, int blocks, int block, cudaStream_t st)
@@ -36,7 +51,8 @@ cudaError_t decode_kernel_launch(const DecodeArgs &a, int blocks, int block, cud
     DecodeArgs b = a;
     int smem = stage_smem_bytes(block, a.width);
     b.stage = smem > 0;
-    k_decode_chains<<<blocks, block, (size_t)smem, st>>>(b);
+    if (dense_instance(a.width)) k_decode_chains<3><<<blocks, block, (size_t)smem, st>>>(b);
+    else k_decode_chains<1><<<blocks, block, (size_t)smem, st>>>(b);
     return cudaGetLastError();
 }
 

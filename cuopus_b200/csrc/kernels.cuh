@@ -106,11 +106,10 @@ __device__ __forceinline__ unsigned queue_next(const DecodeArgs &a, int light)
     return v < K ? v : n;
 }
 
-// Resident 128-thread blocks per SM the register allocation is sized for.
-#ifndef CUO_MIN_BLOCKS
-#define CUO_MIN_BLOCKS 1
-#endif
-__global__ void __launch_bounds__(128, CUO_MIN_BLOCKS) k_decode_chains(DecodeArgs a)
+// MIN_BLOCKS: resident 128-thread blocks per SM the register allocation is
+// sized for (decode_kernel.cu instantiates 1 and 3 and says which runs when).
+template <int MIN_BLOCKS>
+__global__ void __launch_bounds__(128, MIN_BLOCKS) k_decode_chains(DecodeArgs a)
 {
     const int W = a.width;
     const int lane = threadIdx.x & 31;

@@ -44,6 +44,15 @@ def test_int16_results_alone_equal_results_in_the_mix(cuda):
             ids.append(srv.submit(f))
             if i % 3 == 2:
                 time.sleep(0.01)
+        # the server's own size of each request: samples per channel and channels as the probe gives
+        import ctypes
+        from cuopus_b200.serving import _lib
+        for f, rid in zip(files, ids):
+            n, ch, nb = ctypes.c_int64(0), ctypes.c_int32(0), ctypes.c_size_t(0)
+            assert _lib().cuopus_server_request_size(srv._h, rid, ctypes.byref(n), ctypes.byref(ch),
+                                                     ctypes.byref(nb)) == 0
+            assert (n.value, ch.value) == cn.probe_pcm(f) and nb.value == 2 * n.value * ch.value
+        assert _lib().cuopus_server_request_size(srv._h, 10 ** 9, None, None, None) == 3
         for i, rid in enumerate(ids):
             out, ch, lat = srv.wait(rid)
             assert lat > 0
