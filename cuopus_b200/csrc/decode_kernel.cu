@@ -31,7 +31,8 @@ namespace cuo {
 // for 3 resident 128-thread blocks (at most 170 registers, so 12 warps per SM
 // at 64-thread blocks instead of 8), whose chains each decode slower (spills)
 // but more of them are in flight: the 2 h file in 1 s chains at 8 lanes,
-// 179-180 ms against 188-189 (same box, alternating).  Wider groups decode the
+// 179-180 ms against 188-189 (same box, alternating; sized for 4 blocks, 128
+// registers, 239 ms: the spills outweigh the extra warps).  Wider groups decode the
 // long chains that set an uneven batch's step, with few warps per SM: they
 // run the instance with the full register budget (255), which decodes each
 // chain faster (the mixed batch at 5 warps per SM: 2,401-2,496 ms against
