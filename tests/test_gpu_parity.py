@@ -356,3 +356,30 @@ def test_visiting_order_keeps_the_bits(cuda, monkeypatch):
     assert all(np.array_equal(x, y) for x, y in zip(a[0], b[0]))
     assert np.array_equal(a[1], b[1])
     assert a[2] == b[2] == 8
+
+
+@pytest.mark.gpu
+def test_packet_staging_off_keeps_the_bits(cuda, monkeypatch):
+    """CUOPUS_STAGE=0 (packets read in place instead of staged in shared
+    memory) decodes the same samples, at 32 lanes per chain (whole streams,
+    the full-register kernel instance) and at 8 (1 s chains, the 12-warp
+    instance), packets larger than a staging buffer included."""
+    from cuopus_b200 import cuopus_native as cn
+    streams = _streams("mixed", 6, 4.0, 8800)
+    big = corpus.make_stream(dict(kind="mixed", seed=8900, seconds=6.0, channels=2))
+    # some packets exceed a staging buffer (480 bytes) and are read in place either way
+    assert any(len(p) > 480 for f in streams + [big] for p in ogg_port.demux(f)["packets"])
+    got = {}
+    for stage in (None, "0"):
+        if stage:
+            monkeypatch.setenv("CUOPUS_STAGE", stage)
+        else:
+            monkeypatch.delenv("CUOPUS_STAGE", raising=False)
+        out = []
+        for seg, stride in (("1e9", "32"), ("1.0", "8")):
+            monkeypatch.setenv("CUOPUS_SEG_S", seg)
+            monkeypatch.setenv("CUOPUS_STRIDE", stride)
+            out.append([t.cpu().numpy() for t, _ in cn.decode_ogg_to_int16(streams + [big])])
+        got[stage] = out
+    for a, b in zip(got[None], got["0"]):
+        assert all(np.array_equal(x, y) for x, y in zip(a, b))
