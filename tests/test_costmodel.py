@@ -109,14 +109,18 @@ def test_gpu_forward_and_gradient_match_oracle(cuda):
 
 
 @pytest.mark.gpu
-def test_gpu_training_learns_decode_cost_and_beats_packet_order(cuda):
+def test_gpu_training_learns_decode_cost(cuda):
     """Record per-chain decode cycles on a mixed batch, train on half, and
     evaluate on the other half against the fallback (packets x channels, fitted
     to log cycles by least squares on the same half):
       * the network explains more of the variance of log cycles;
       * predicting the makespan of a longest-first schedule from the predicted
         costs, its error is smaller than the fallback's;
-      * its longest-first schedule is no worse than the fallback's beyond 10 %."""
+      * its longest-first schedule's makespan is the fallback's within 2 %: on
+        a batch of whole streams the longest chains set the makespan of any
+        longest-first order, so the better prediction does not shorten it
+        (where the order does decide the step -- 1 s chains of a long file,
+        about 1.5 chains per decoder group -- the bench measures the gain)."""
     from cuopus_b200 import costmodel
     from gpu_util import device_batch, run_device_batch
     from oracle import corpus
@@ -162,4 +166,4 @@ def test_gpu_training_learns_decode_cost_and_beats_packet_order(cuda):
           "makespan mlp %.4g / packets %.4g" % (r2, r2_pkt, err_mlp, err_pkt, ms_mlp, ms_pkt))
     assert r2 > 0.7 and r2 > r2_pkt
     assert err_mlp < err_pkt
-    assert ms_mlp <= 1.10 * ms_pkt
+    assert ms_mlp <= 1.02 * ms_pkt
